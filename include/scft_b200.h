@@ -1,0 +1,154 @@
+/*
+ * scft_b200.h -- C ABI of the B200 (sm_100a) SCFT string-method field solver.
+ *
+ * Drop-in boundary for the hot path of PolymerTheory/SCFT_string: the
+ * Richardson pseudo-spectral propagator, the composite-Simpson density sum,
+ * the field mixing and the cubic-spline string reparametrisation
+ * (solve_field and what it calls).  Plain C types only; every function
+ * returns a status and never exits the process (the reference calls
+ * exit(EXIT_FAILURE) on any CUDA error, GPU_kernels.h:16-48).
+ *
+ * Conventions (identical to the reference):
+ *   grid point  r = z + m2*(y + m1*x)                    (scft.cu:462-464)
+ *   replica fields are host arrays of doubles: [W-, W+] (2*M) and the
+ *   concentrations [phiA, phiB, phih, phicB] (4*M)   (scft.cu:1037-1051)
+ *
+ * Ownership and threading: a context owns one CUDA stream and all device
+ * memory it uses; the caller owns every host buffer.  A context is not
+ * thread-safe; separate contexts may be used from separate threads.
+ * The library runs only on sm_100a (B200); there is no CPU fallback.
+ */
+#ifndef SCFT_B200_H
+#define SCFT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SCFT_OK = 0,
+    SCFT_CUDA_ERROR = 1,     /* a CUDA call failed; see scft_last_error */
+    SCFT_NAN_DETECTED = 2,   /* a residual became NaN (the reference asserts, scft.cu:539) */
+    SCFT_BAD_INPUT = 3,      /* invalid argument or unsupported size */
+    SCFT_TIMEOUT = 4,        /* a bounded device wait gave up */
+    SCFT_OUT_OF_MEMORY = 5,
+    SCFT_UNSUPPORTED = 6     /* no sm_100a device */
+} scft_status;
+
+typedef enum { SCFT_FP64 = 0, SCFT_FP32 = 1 } scft_precision;
+
+/* Problem definition: the input.dat keys of the reference (scft.cu:120-251)
+ * plus the replica count (compile-time `strn` in the reference, scft.cu:35). */
+typedef struct {
+    int    m[3];        /* mesh points per axis */
+    double D[3];        /* box lengths in units of R0 */
+    int    N;           /* contour steps of the copolymer */
+    double alpha;       /* homopolymer/copolymer length ratio (Nh = (int)(alpha*N)) */
+    int    ens;         /* 1 canonical, 2 grand canonical */
+    double phidb;       /* copolymer volume fraction (ens 1) or fugacity (ens 2) */
+    double chi;         /* chi*N */
+    double f;           /* A fraction of the copolymer; rounded to round(N f)/N as scft.cu:1008 */
+    int    strn;        /* replicas on the string, 1..64 */
+    int    fix[2];      /* keep the first / last replica fixed */
+    int    dostring;    /* 1: string method, 0: independent replicas */
+    int    springsteps; /* initial iterations with spring coupling (missing win files) */
+    int    precision;   /* scft_precision of the propagator bulk (reductions are FP64) */
+    int    batched;     /* 1: all replicas advance together; 0: one replica at a time */
+    int    device;      /* CUDA device ordinal */
+} scft_problem;
+
+typedef struct scft_ctx scft_ctx;
+
+/* One record per solve_field iteration (scft.cu:592-806). */
+typedef struct {
+    int    k;
+    double lambda;
+    double errtot;      /* sqrt(mean over replicas of errs3^2), scft.cu:764-765 */
+    double fitup;
+    double stepav;      /* mean props calls per replica in this iteration */
+    int    did_freee;   /* FreeE ran at the end of this iteration (k % 50 == 0 or last) */
+    double FE;          /* total free energy of that FreeE */
+} scft_iter_report;
+
+typedef struct {
+    long long props_calls;    /* replica props evaluations */
+    long long contour_steps;  /* replica contour steps (Ns per props) */
+    long long kernel_launches;
+    double    props_seconds;  /* device time of props batches (CUDA events) */
+} scft_stats;
+
+/* ---- lifetime --------------------------------------------------------- */
+/* Replaces `new density(N, D)` + setupSplineBuffers (scft.cu:1010-1011,
+ * density.h:272-315, 462-476). */
+scft_status scft_create(const scft_problem *p, scft_ctx **out);
+void        scft_destroy(scft_ctx *ctx);
+const char *scft_last_error(const scft_ctx *ctx);
+const char *scft_status_string(scft_status s);
+
+/* ---- fields ----------------------------------------------------------- */
+/* Replica ii's [W-, W+] (2*M doubles): the first 2*M entries of W[ii]
+ * (scft.cu:1062). */
+scft_status scft_set_fields(scft_ctx *ctx, int ii, const double *w2M);
+scft_status scft_get_fields(const scft_ctx *ctx, int ii, double *w2M);
+/* Concentrations of the last props of replica ii: [phiA, phiB, phih, phicB]
+ * (4*M doubles, W[ii]+2M of the reference), lnQ and phis[5]. */
+scft_status scft_get_conc(const scft_ctx *ctx, int ii, double *out4M, double *lnQ, double *phis);
+/* Replica ownership mask of the single process (doiis, scft.cu:953-975). */
+scft_status scft_get_doiis(const scft_ctx *ctx, int *doiis);
+
+/* ---- density ---------------------------------------------------------- */
+/* density::props on the device-resident fields of replica ii
+ * (density.h:344-459). */
+scft_status scft_props(scft_ctx *ctx, int ii);
+/* density::props with the reference's host-pointer signature
+ * (density.h:344): w[0:2M) in, w[2M:6M) out; ii is unused as in the
+ * reference; Ns, alpha, phic and f must match the context (BAD_INPUT
+ * otherwise). */
+scft_status scft_props_host(scft_ctx *ctx, double *w, double *lnQ, int ii, int Ns, double alpha,
+                            double phic, double *phis, double f);
+/* One Richardson contour step (step::do_step, density.h:129-220) of the
+ * host slice in = [q, q^dagger] (2*M doubles) for the fields of replica ii
+ * -> out (2*M doubles). */
+scft_status scft_do_step(scft_ctx *ctx, int ii, const double *in, double *out, int s);
+/* Propagator slice of the last props of replica ii: which 0 = q(s), 1 = q^dagger(s). */
+scft_status scft_get_propagator(const scft_ctx *ctx, int ii, int which, int s, double *outM);
+
+/* ---- solvers ---------------------------------------------------------- */
+/* solve_field0 (scft.cu:516-554) on replica ii; *k_out = the reference's k. */
+scft_status scft_solve_field0(scft_ctx *ctx, int ii, int maxIter, double errTol, int *k_out);
+/* W+ relaxation of every replica (the prelude of main, scft.cu:1105). */
+scft_status scft_solve_field0_all(scft_ctx *ctx, int maxIter, double errTol, int *k_out);
+/* solve_field (scft.cu:559-809), doii = -1 for the whole string.  reports
+ * (maxIter entries), errs and errs3 (maxIter*strn doubles) may be NULL. */
+scft_status scft_solve_field(scft_ctx *ctx, int doii, int maxIter, double errTol,
+                             scft_iter_report *reports, double *errs, double *errs3, int *k_out);
+/* Iteration-at-a-time form of scft_solve_field: begin, then step until the
+ * reference loop would stop (*done set), then end. */
+scft_status scft_string_begin(scft_ctx *ctx, int doii, int maxIter, double errTol);
+scft_status scft_string_step(scft_ctx *ctx, scft_iter_report *rep, double *errs, double *errs3,
+                             int *done);
+scft_status scft_string_end(scft_ctx *ctx, int *k_out);
+/* FreeE (scft.cu:812-853): W+ re-solve (100 iterations, 1e-4) and props of
+ * every replica, then F = -lnQ + <chi phiA phiB - wA phiA - wB phiB>.
+ * Arrays have strn entries; any may be NULL. */
+scft_status scft_free_energy(scft_ctx *ctx, double *FE, double *FEs, double *FEs0, double *FEs1,
+                             double *phctot, double *alf);
+
+/* ---- string spline services (host pointers) --------------------------- */
+/* density::splineDerivsChunked (density.h:491-508): ww[ii] -> W- of replica
+ * ii; out[ii][r0..r0+n) = dW-/dalpha at knot x[ii] for doiis[ii] == 1. */
+scft_status scft_spline_derivs(scft_ctx *ctx, const double *x, const double *const *ww, int r0,
+                               int n, const int *doiis, double *const *out);
+/* density::splineRedistChunked (density.h:511-528): ww[ii][r] += lambda *
+ * (S(xref[ii]) - ww[ii][r]) for interior replicas with doiis[ii] == 1. */
+scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xref,
+                               double *const *ww, int r0, int n, const int *doiis, double lambda);
+
+/* ---- statistics ------------------------------------------------------- */
+scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
+scft_status scft_reset_stats(scft_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

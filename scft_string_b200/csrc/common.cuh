@@ -1,0 +1,61 @@
+// common.cuh -- shared types of the sm_100a SCFT kernels.
+//
+// Layouts (same as the reference, scft.cu:462-464 and density.h:90):
+//   real grid      r = z + m2*(y + m1*x)
+//   half spectrum  k = kz + mk2*(ky + m1*kx),  mk2 = m2/2 + 1
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scft {
+
+template <typename T>
+struct cplx {
+    T x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b)
+{
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// a * conj(b)
+template <typename T>
+__device__ __forceinline__ cplx<T> cmulc(cplx<T> a, cplx<T> b)
+{
+    return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b)
+{
+    return {a.x + b.x, a.y + b.y};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b)
+{
+    return {a.x - b.x, a.y - b.y};
+}
+
+constexpr int kMaxStages = 12;
+constexpr int kPairLanes = 8;  // slab pack/unpack: mk2 <= 32*kPairLanes
+
+// Mixed-radix factorisation of one FFT length (radices 2, 3, 4, 5, 7, 8).
+struct Plan1D {
+    int n;
+    int nst;
+    int radix[kMaxStages];
+};
+
+// Everything a propagator kernel needs to know about the grid.
+struct Geo {
+    int m0, m1, m2, mk2;
+    int M, Mk;
+    int npair;       // ceil(m1/2): packed real y-line pairs per x-slab
+    int slab_c;      // complex elements of one slab buffer (m1*mk2 + slack)
+    Plan1D px, py, pz;
+    int Ns, n1, n2, Nh;
+    int ncol_tiles;  // x-pencil tiles per field
+    int tc;          // columns per x-pencil tile
+};
+
+}  // namespace scft

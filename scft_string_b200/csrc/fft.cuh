@@ -1,0 +1,328 @@
+// fft.cuh -- CTA-wide mixed-radix FFTs on shared memory for sm_100a.
+//
+// This replaces the cuFFT D2Z/Z2D plans of the reference (density.h:67-74,
+// 149-205).  A 3-D real transform of one field is split into
+//   * an x-slab pass (one CTA per x index): the real m1 x m2 slab is packed as
+//     ceil(m1/2) complex rows (y-line pairs), z-transformed, unpacked into the
+//     m1 x (m2/2+1) half spectrum and y-transformed -- all in shared memory;
+//   * an x-pencil pass (one CTA per tile of consecutive (ky, kz) columns) that
+//     transforms along x, applies the diffusion factor and transforms back.
+// The inverse runs the slab pass backwards.
+//
+// Each 1-D FFT is a Stockham autosort transform: stage (radix R, accumulated
+// size Ns) reads element j + r*n/R of a line, multiplies by
+// exp(sign*2*pi*i*r*(j%Ns)/(Ns*R)), does an R-point DFT in registers and
+// writes element (j/Ns)*Ns*R + j%Ns + r*Ns.  Stages run in place: every thread
+// stages its butterflies in registers across one __syncthreads.
+// Twiddles come from a table exp(-2*pi*i*t/n) computed on the host in FP64.
+#pragma once
+#include "common.cuh"
+
+namespace scft {
+
+// multiply by sign*i
+template <typename T>
+__device__ __forceinline__ cplx<T> mul_si(cplx<T> a, int sign)
+{
+    return sign > 0 ? cplx<T>{-a.y, a.x} : cplx<T>{a.y, -a.x};
+}
+
+// R-point DFTs in registers: V[q] = sum_r v[r] exp(sign*2*pi*i*r*q/R).
+template <typename T, int R>
+struct Dft;
+
+template <typename T>
+struct Dft<T, 2> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int, const cplx<T> *, int)
+    {
+        cplx<T> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <typename T>
+struct Dft<T, 4> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int sign, const cplx<T> *, int)
+    {
+        cplx<T> a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        cplx<T> c = cadd(v[1], v[3]), d = mul_si(csub(v[1], v[3]), sign);
+        v[0] = cadd(a, c);
+        v[1] = cadd(b, d);
+        v[2] = csub(a, c);
+        v[3] = csub(b, d);
+    }
+};
+
+template <typename T>
+struct Dft<T, 8> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int sign, const cplx<T> *, int)
+    {
+        const T c = (T)0.70710678118654752440;  // sqrt(1/2)
+        const T s = (T)sign;
+        cplx<T> e[4] = {v[0], v[2], v[4], v[6]};
+        cplx<T> o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<T, 4>::run(e, sign, nullptr, 0);
+        Dft<T, 4>::run(o, sign, nullptr, 0);
+        // o[k] *= exp(sign*2*pi*i*k/8)
+        cplx<T> o1 = {c * (o[1].x - s * o[1].y), c * (o[1].y + s * o[1].x)};
+        cplx<T> o2 = mul_si(o[2], sign);
+        cplx<T> o3 = {c * (-o[3].x - s * o[3].y), c * (-o[3].y + s * o[3].x)};
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
+    }
+};
+
+template <typename T>
+struct Dft<T, 3> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int sign, const cplx<T> *, int)
+    {
+        const T h = (T)0.86602540378443864676;  // sqrt(3)/2
+        cplx<T> t1 = cadd(v[1], v[2]);
+        cplx<T> m = {v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
+        cplx<T> d = mul_si(csub(v[1], v[2]), sign);
+        d.x *= h;
+        d.y *= h;
+        v[0] = cadd(v[0], t1);
+        v[1] = cadd(m, d);
+        v[2] = csub(m, d);
+    }
+};
+
+template <typename T>
+struct Dft<T, 5> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int sign, const cplx<T> *, int)
+    {
+        const T c1 = (T)0.30901699437494742410;   // cos(2 pi/5) = (sqrt5 - 1)/4
+        const T c2 = (T)-0.80901699437494742410;  // cos(4 pi/5) = -(sqrt5 + 1)/4
+        const T s1 = (T)0.95105651629515357212;   // sin(2 pi/5)
+        const T s2 = (T)0.58778525229247312917;   // sin(4 pi/5)
+        cplx<T> a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
+        cplx<T> b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
+        cplx<T> r1 = {v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y};
+        cplx<T> r2 = {v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y};
+        cplx<T> i1 = mul_si(cplx<T>{s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y}, sign);
+        cplx<T> i2 = mul_si(cplx<T>{s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y}, sign);
+        v[0] = {v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y};
+        v[1] = cadd(r1, i1);
+        v[4] = csub(r1, i1);
+        v[2] = cadd(r2, i2);
+        v[3] = csub(r2, i2);
+    }
+};
+
+// direct DFT for radix 7 with roots taken from the length-n table
+template <typename T>
+struct Dft<T, 7> {
+    static __device__ __forceinline__ void run(cplx<T> *v, int sign, const cplx<T> *tw, int n)
+    {
+        const int step = n / 7;
+        cplx<T> out[7];
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            cplx<T> acc = v[0];
+#pragma unroll
+            for (int r = 1; r < 7; r++) {
+                cplx<T> w = tw[((r * q) % 7) * step];
+                acc = cadd(acc, sign < 0 ? cmul(v[r], w) : cmulc(v[r], w));
+            }
+            out[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < 7; q++) v[q] = out[q];
+    }
+};
+
+// Elements a thread stages in registers per stage (complex values).
+constexpr int kStageBudget = 16;
+
+template <int R>
+struct Slots {
+    static constexpr int value = kStageBudget / R;
+};
+
+// One Stockham stage over `nlines` lines of length n.  Element i of line l is
+// buf[l*ls + i*es].  line_fast selects the butterfly->thread order: consecutive
+// threads walk lines (good when ls == 1) or butterflies (good when es == 1).
+template <typename T, int R>
+__device__ __noinline__ void fft_stage(cplx<T> *__restrict__ buf, int n, int nlines, int es,
+                                     int ls, bool line_fast, int Ns,
+                                     const cplx<T> *__restrict__ tw, int sign, int *err)
+{
+    constexpr int SL = Slots<R>::value;
+    const int nR = n / R;
+    const int nb = nlines * nR;
+    const int tstep = n / (Ns * R);
+    const int nthr = blockDim.x;
+    cplx<T> v[SL][R];
+#pragma unroll
+    for (int sl = 0; sl < SL; sl++) {
+        const int b = threadIdx.x + sl * nthr;
+        if (b < nb) {
+            int line, j;
+            if (line_fast) {
+                line = b % nlines;
+                j = b / nlines;
+            } else {
+                j = b % nR;
+                line = b / nR;
+            }
+            const int k = j % Ns;
+            const cplx<T> *src = buf + line * ls + j * es;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                cplx<T> a = src[r * nR * es];
+                if (r > 0 && k > 0) {
+                    const cplx<T> w = tw[r * k * tstep];
+                    a = sign < 0 ? cmul(a, w) : cmulc(a, w);
+                }
+                v[sl][r] = a;
+            }
+            Dft<T, R>::run(v[sl], sign, tw, n);
+        }
+    }
+    if (threadIdx.x + SL * nthr < nb) *err = 1;  // launch geometry too small: host bug
+    __syncthreads();
+#pragma unroll
+    for (int sl = 0; sl < SL; sl++) {
+        const int b = threadIdx.x + sl * nthr;
+        if (b < nb) {
+            int line, j;
+            if (line_fast) {
+                line = b % nlines;
+                j = b / nlines;
+            } else {
+                j = b % nR;
+                line = b / nR;
+            }
+            const int k = j % Ns;
+            cplx<T> *dst = buf + line * ls + ((j - k) * R + k) * es;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[r * Ns * es] = v[sl][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void cta_fft(cplx<T> *buf, const Plan1D &p, int nlines, int es, int ls, bool line_fast,
+                        const cplx<T> *tw, int sign, int *err)
+{
+    int Ns = 1;
+    for (int st = 0; st < p.nst; st++) {
+        const int R = p.radix[st];
+        switch (R) {
+            case 8: fft_stage<T, 8>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            case 4: fft_stage<T, 4>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            case 2: fft_stage<T, 2>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            case 3: fft_stage<T, 3>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            case 5: fft_stage<T, 5>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            case 7: fft_stage<T, 7>(buf, p.n, nlines, es, ls, line_fast, Ns, tw, sign, err); break;
+            default: *err = 2; return;
+        }
+        Ns *= R;
+    }
+}
+
+// After the forward z-transform of packed rows C = FFT(a[2p] + i a[2p+1]):
+// A[k] = (C[k] + conj C[-k])/2 and B[k] = (C[k] - conj C[-k])/(2i) are the half
+// spectra of the two real lines; they go to rows 2p and 2p+1 of the slab.
+// One warp per pair; reads and writes stay inside the pair's own rows.
+template <typename T>
+__device__ void slab_unpack(cplx<T> *buf, const Geo &g)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int m2 = g.m2, mk2 = g.mk2;
+    for (int p = warp; p < g.npair; p += nw) {
+        cplx<T> *row = buf + 2 * p * mk2;
+        const bool has_b = (2 * p + 1 < g.m1);
+        cplx<T> A[kPairLanes], B[kPairLanes];
+#pragma unroll
+        for (int t = 0; t < kPairLanes; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < mk2) {
+                const cplx<T> ck = row[kz];
+                const cplx<T> cm = row[kz == 0 ? 0 : m2 - kz];
+                A[t] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
+                B[t] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kPairLanes; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < mk2) {
+                row[kz] = A[t];
+                if (has_b) row[mk2 + kz] = B[t];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Inverse of slab_unpack with half-complex-to-real semantics: the imaginary
+// parts of the self-conjugate bins (kz = 0 and kz = m2/2) are dropped, and
+// C[k] = A[k] + i B[k], C[-k] = conj A[k] + i conj B[k].
+template <typename T>
+__device__ void slab_pack(cplx<T> *buf, const Geo &g)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int m2 = g.m2, mk2 = g.mk2;
+    for (int p = warp; p < g.npair; p += nw) {
+        cplx<T> *row = buf + 2 * p * mk2;
+        const bool has_b = (2 * p + 1 < g.m1);
+        cplx<T> A[kPairLanes], B[kPairLanes];
+#pragma unroll
+        for (int t = 0; t < kPairLanes; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < mk2) {
+                A[t] = row[kz];
+                B[t] = has_b ? row[mk2 + kz] : cplx<T>{(T)0, (T)0};
+                if (kz == 0 || 2 * kz == m2) {
+                    A[t].y = (T)0;
+                    B[t].y = (T)0;
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kPairLanes; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < mk2) {
+                row[kz] = {A[t].x - B[t].y, A[t].y + B[t].x};
+                if (kz > 0 && 2 * kz < m2) row[m2 - kz] = {A[t].x + B[t].y, B[t].x - A[t].y};
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// packed real rows -> half spectrum [y][kz]
+template <typename T>
+__device__ void slab_forward(cplx<T> *buf, const Geo &g, const cplx<T> *twy, const cplx<T> *twz,
+                             int *err)
+{
+    cta_fft(buf, g.pz, g.npair, 1, 2 * g.mk2, false, twz, -1, err);
+    slab_unpack(buf, g);
+    __syncthreads();
+    cta_fft(buf, g.py, g.mk2, g.mk2, 1, true, twy, -1, err);
+}
+
+// half spectrum [y][kz] -> packed real rows (unnormalised)
+template <typename T>
+__device__ void slab_inverse(cplx<T> *buf, const Geo &g, const cplx<T> *twy, const cplx<T> *twz,
+                             int *err)
+{
+    cta_fft(buf, g.py, g.mk2, g.mk2, 1, true, twy, +1, err);
+    slab_pack(buf, g);
+    __syncthreads();
+    cta_fft(buf, g.pz, g.npair, 1, 2 * g.mk2, false, twz, +1, err);
+}
+
+}  // namespace scft

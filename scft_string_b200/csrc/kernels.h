@@ -1,0 +1,100 @@
+// kernels.h -- launch interfaces between the host solver (scft_ctx.cu) and the
+// sm_100a kernels (props_kernels.cu, field_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace scft {
+
+// per-replica scalar record in device memory (doubles)
+enum {
+    kRsQ2 = 0,
+    kRsQC = 1,
+    kRsLnQ = 2,
+    kRsZB = 3,
+    kRsZC = 4,
+    kRsPhis = 5,  // 5 values
+    kRsDev2 = 10, // sum over M of (chi*(phiA+phiB-1))^2 of the last props
+    kRsStride = 16
+};
+
+// Arguments of every propagator kernel (passed by value).
+template <typename T>
+struct PropsArgs {
+    Geo g;
+    const int *slot_rep;    // slot -> replica index
+    const double *W;        // [rep][2M]  W-, W+
+    double *conc;           // [rep][4M]  phiA, phiB, phih, phicB
+    double *rs;             // [rep][kRsStride]
+    T *etab;                // [slot][2][M]  exp(-wA ds/4), exp(-wB ds/4)
+    T *hist;                // [slot][Ns+1][2][M]  q(s), q^dagger(s)
+    cplx<T> *spec;          // [slot][2 fields][2 spectra][Mk]
+    T *pbuf;                // [slot][2][M]  E2 * full-step result
+    const cplx<T> *tw;      // twiddles: x (m0) | y (m1) | z (m2)
+    const T *kfac;          // per-axis diffusion factors: x (m0) | y (m1) | z (mk2)
+    double *partials;       // [slot][npart_stride]
+    int npart_stride;
+    T invM, Mreal;
+    double chi, phic, alpha;
+    int ens;
+    int *err;               // device error word (launch-geometry / plan errors)
+};
+
+struct PropsLaunch {
+    int slab_threads, slab_smem;
+    int pencil_threads, pencil_smem;
+    int ew_blocks;   // elementwise grid (per slot)
+    int red_blocks;  // reduction grid (per slot)
+    int big;         // FFT kernels need more than 256 threads per CTA
+};
+
+template <typename T>
+int launch_props(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st);
+template <typename T>
+int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st);
+template <typename T>
+int set_props_smem(const PropsLaunch &L);
+
+// ------------------------------------------------------------------ FP64 field kernels
+constexpr int kMaxStrn = 64;
+
+struct FieldArgs {
+    int M;
+    int strn;
+    const int *rep_list;   // replicas processed by the launch (blockIdx.y)
+    double *W;             // [rep][2M]
+    const double *conc;    // [rep][4M]
+    double *DEV;           // [rep][2M]
+    double *dWda;          // [rep][M]
+    double *partials;      // [slotq][nblk]
+    double chi;
+};
+
+// coefficients of the natural cubic spline that depend on the knots only
+struct SplineKnots {
+    int strn;
+    double h[kMaxStrn], l[kMaxStrn], u[kMaxStrn];
+    int nm_d[kMaxStrn];     // interval of knot ev (derivative evaluation)
+    double dx_d[kMaxStrn];
+    int nm_v[kMaxStrn];     // interval of xref[ev] (value evaluation)
+    double dx_v[kMaxStrn];
+    int doiis[kMaxStrn];
+};
+
+void launch_dev(const FieldArgs &a, int nrep_launch, int nblk, int dospring, double eps,
+                cudaStream_t st);
+void launch_mix0(const FieldArgs &a, int nrep_launch, const double *lam, cudaStream_t st);
+void launch_mix(const FieldArgs &a, double lambda, cudaStream_t st);
+void launch_edist(const FieldArgs &a, int nblk, cudaStream_t st);
+void launch_spline_deriv(const FieldArgs &a, const SplineKnots *knots, int nblk, cudaStream_t st);
+void launch_dots(const FieldArgs &a, int nrep_launch, int nblk, cudaStream_t st);
+void launch_perp(const FieldArgs &a, int nrep_launch, const double *coef, const double *ndev,
+                 int nblk, cudaStream_t st);
+void launch_redist(const FieldArgs &a, const SplineKnots *knots, double lambda, int nblk,
+                   cudaStream_t st);
+void launch_freee(const FieldArgs &a, int nrep_launch, double f, int nblk, cudaStream_t st);
+void launch_reduce_final(const double *partials, int nrows, int nblk, double *out,
+                         cudaStream_t st);
+
+}  // namespace scft

@@ -1,0 +1,501 @@
+// props_kernels.cu -- the contour-step pipeline of density::props on sm_100a.
+//
+// One Richardson step (density.h:129-220, GPU_kernels.h:175-203) advances q and
+// q^dagger of every replica slot in the batch:
+//   qs0 = IFFT(K2 FFT(E2 * IFFT(K2 FFT(E4 q))))      (two half steps)
+//   qs1 = IFFT(K1 FFT(E2 q))                        (one full step)
+//   q'  = (4 E4 qs0 - E2 qs1) / 3
+// with E4 = exp(-w ds/4), E2 = E4^2, K2 = exp(-k^2 ds/12)/M, K1 = K2^2 M.
+// Four launches per step, each over (slot, field, slab-or-tile):
+//   pencil(both)  x-transform of the two spectra, times K2 / K1, back
+//   mid           inverse slab of qs1 -> P = E2 qs1 (real, kept for the
+//                 combine); inverse slab of the half step, times E2, forward
+//   pencil(A)     x-transform, times K2, back
+//   combine       inverse slab -> q' = (4 E4 qs0 - P)/3 -> propagator store;
+//                 forward slabs of E4' q' and E2' q' for the next step
+// The q(s) store (density.h:293-301 keeps every slice) feeds the Simpson
+// density pass (density.h:402-430), done by k_density in FP64.
+#include "common.cuh"
+#include "fft.cuh"
+#include "kernels.h"
+
+namespace scft {
+
+template <typename T>
+__device__ __forceinline__ size_t hist_off(const Geo &g, int slot, int s, int fld)
+{
+    return (((size_t)slot * (g.Ns + 1) + s) * 2 + fld) * (size_t)g.M;
+}
+
+// E4 table (0: A field, 1: B field) for field fld (0: q, 1: q^dagger) at step s;
+// q sees the A block for s < n1, q^dagger the B block for s < n2 (density.h:136-146)
+__device__ __forceinline__ int etab_sel(const Geo &g, int fld, int s)
+{
+    return fld == 0 ? (s < g.n1 ? 0 : 1) : (s < g.n2 ? 1 : 0);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_tw(cplx<T> *dst, const cplx<T> *src, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------- prepare
+// E4 = exp(-wA ds/4), exp(-wB ds/4) with wA = W- + W+, wB = W+ - W-
+// (Prepare_dev_dev_expWds2_dev_expWds, GPU_kernels.h:215-225)
+template <typename T>
+__global__ void k_prepare(PropsArgs<T> a)
+{
+    const Geo g = a.g;
+    const int slot = blockIdx.y;
+    const int rep = a.slot_rep[slot];
+    const double *W = a.W + (size_t)rep * 2 * g.M;
+    T *e = a.etab + (size_t)slot * 2 * g.M;
+    const double ds = 1.0 / g.Ns;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < g.M; r += gridDim.x * blockDim.x) {
+        const double wm = W[r], wp = W[r + g.M];
+        e[r] = (T)exp(-(wm + wp) * ds / 4);
+        e[r + g.M] = (T)exp(-(-wm + wp) * ds / 4);
+    }
+}
+
+// ---------------------------------------------------------------- combine
+// mode 0: finishes step s (q(s+1) = Richardson combination);
+// mode 1: q(s+1) = 1 (Array_set_value, density.h:368-369; called with s = -1);
+// mode 2: q(s+1) is taken from the propagator store (single-step entry).
+// Then starts step s+1 when s+1 < Ns.
+template <typename T, int MT>
+__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> a, int s, int mode)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const Geo &g = a.g;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *twy = buf + g.slab_c;
+    cplx<T> *twz = twy + g.m1;
+    load_tw(twy, a.tw + g.m0, g.m1);
+    load_tw(twz, a.tw + g.m0 + g.m1, g.m2);
+    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2, M = g.M;
+    const size_t slab_r = (size_t)x * m1 * m2;  // real offset of this slab
+    const size_t slab_k = (size_t)x * m1 * mk2;
+    const T *etab = a.etab + (size_t)slot * 2 * M;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
+    cplx<T> *specB = specA + g.Mk;
+    const int sn = s + 1;
+    T *qn = a.hist + hist_off<T>(g, slot, sn, fld) + slab_r;
+    const int npz = g.npair * m2;
+
+    if (mode == 0) {
+        for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specA[slab_k + i];
+        __syncthreads();
+        slab_inverse(buf, g, twy, twz, a.err);
+        const T *E4 = etab + (size_t)etab_sel(g, fld, s) * M + slab_r;
+        const T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
+        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+            const int p = e / m2, z = e - p * m2;
+            cplx<T> &c = buf[2 * p * mk2 + z];
+            const int r0 = 2 * p * m2 + z;
+            // Richardson, GPU_kernels.h:199-203
+            c.x = (c.x * E4[r0] * (T)4 - P[r0]) / (T)3;
+            qn[r0] = c.x;
+            if (2 * p + 1 < m1) {
+                const int r1 = r0 + m2;
+                c.y = (c.y * E4[r1] * (T)4 - P[r1]) / (T)3;
+                qn[r1] = c.y;
+            } else {
+                c.y = (T)0;
+            }
+        }
+    } else if (mode == 1) {
+        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+            const int p = e / m2, z = e - p * m2;
+            const int r0 = 2 * p * m2 + z;
+            const bool hb = 2 * p + 1 < m1;
+            buf[2 * p * mk2 + z] = {(T)1, hb ? (T)1 : (T)0};
+            qn[r0] = (T)1;
+            if (hb) qn[r0 + m2] = (T)1;
+        }
+    } else {
+        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+            const int p = e / m2, z = e - p * m2;
+            const int r0 = 2 * p * m2 + z;
+            const bool hb = 2 * p + 1 < m1;
+            buf[2 * p * mk2 + z] = {qn[r0], hb ? qn[r0 + m2] : (T)0};
+        }
+    }
+    if (sn >= g.Ns) return;
+    __syncthreads();
+    const T *E4n = etab + (size_t)etab_sel(g, fld, sn) * M + slab_r;
+    // half step input E4' q'
+    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        const int p = e / m2, z = e - p * m2;
+        cplx<T> &c = buf[2 * p * mk2 + z];
+        const int r0 = 2 * p * m2 + z;
+        c.x *= E4n[r0];
+        if (2 * p + 1 < m1) c.y *= E4n[r0 + m2];
+    }
+    __syncthreads();
+    slab_forward(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specA[slab_k + i] = buf[i];
+    __syncthreads();
+    // full step input E2' q' (q' re-read from the propagator store written above)
+    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        const int p = e / m2, z = e - p * m2;
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = E4n[r0];
+        T v0 = qn[r0] * (e0 * e0), v1 = (T)0;
+        if (2 * p + 1 < m1) {
+            const T e1 = E4n[r0 + m2];
+            v1 = qn[r0 + m2] * (e1 * e1);
+        }
+        buf[2 * p * mk2 + z] = {v0, v1};
+    }
+    __syncthreads();
+    slab_forward(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specB[slab_k + i] = buf[i];
+}
+
+// ---------------------------------------------------------------- mid
+template <typename T, int MT>
+__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_mid(PropsArgs<T> a, int s)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const Geo &g = a.g;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *twy = buf + g.slab_c;
+    cplx<T> *twz = twy + g.m1;
+    load_tw(twy, a.tw + g.m0, g.m1);
+    load_tw(twz, a.tw + g.m0 + g.m1, g.m2);
+    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2, M = g.M;
+    const size_t slab_r = (size_t)x * m1 * m2;
+    const size_t slab_k = (size_t)x * m1 * mk2;
+    const T *E4 = a.etab + (size_t)slot * 2 * M + (size_t)etab_sel(g, fld, s) * M + slab_r;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
+    cplx<T> *specB = specA + g.Mk;
+    T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
+    const int npz = g.npair * m2;
+
+    // full step: P = E2 * qs1
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specB[slab_k + i];
+    __syncthreads();
+    slab_inverse(buf, g, twy, twz, a.err);
+    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        const int p = e / m2, z = e - p * m2;
+        const cplx<T> c = buf[2 * p * mk2 + z];
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = E4[r0];
+        P[r0] = c.x * (e0 * e0);
+        if (2 * p + 1 < m1) {
+            const T e1 = E4[r0 + m2];
+            P[r0 + m2] = c.y * (e1 * e1);
+        }
+    }
+    __syncthreads();
+    // second half step input: E2 * (first half step)
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specA[slab_k + i];
+    __syncthreads();
+    slab_inverse(buf, g, twy, twz, a.err);
+    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        const int p = e / m2, z = e - p * m2;
+        cplx<T> &c = buf[2 * p * mk2 + z];
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = E4[r0];
+        c.x *= e0 * e0;
+        if (2 * p + 1 < m1) {
+            const T e1 = E4[r0 + m2];
+            c.y *= e1 * e1;
+        } else {
+            c.y = (T)0;
+        }
+    }
+    __syncthreads();
+    slab_forward(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specA[slab_k + i] = buf[i];
+}
+
+// ---------------------------------------------------------------- pencil
+// x-transform of a tile of tc consecutive (ky, kz) columns, times the
+// diffusion factor (Mult_self, GPU_kernels.h:175-181), inverse x-transform.
+// both != 0: spectrum A with K2 and spectrum B with K1; else A with K2 only.
+template <typename T, int MT>
+__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_pencil(PropsArgs<T> a, int both)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const Geo &g = a.g;
+    const int tc = g.tc, m0 = g.m0;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *twx = buf + tc * m0;
+    T *colf = reinterpret_cast<T *>(twx + m0);
+    T *gx = colf + tc;
+    load_tw(twx, a.tw, m0);
+    const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const int ncol = g.m1 * g.mk2;
+    const int c0 = tile * tc;
+    for (int t = threadIdx.x; t < tc; t += blockDim.x) {
+        const int c = c0 + t;
+        const int y = c / g.mk2, kz = c - y * g.mk2;
+        colf[t] = c < ncol ? a.kfac[m0 + y] * a.kfac[m0 + g.m1 + kz] : (T)0;
+    }
+    for (int i = threadIdx.x; i < m0; i += blockDim.x) gx[i] = a.kfac[i];
+    const T invM = a.invM;
+    cplx<T> *spec = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
+    const int npass = both ? 2 : 1;
+    for (int pass = 0; pass < npass; pass++) {
+        cplx<T> *sp = spec + (size_t)pass * g.Mk;
+        __syncthreads();
+        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+            const int x = e / tc, t = e - x * tc;
+            const int c = c0 + t;
+            buf[e] = c < ncol ? sp[(size_t)x * ncol + c] : cplx<T>{(T)0, (T)0};
+        }
+        __syncthreads();
+        cta_fft(buf, g.px, tc, tc, 1, true, twx, -1, a.err);
+        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+            const int x = e / tc, t = e - x * tc;
+            const T k2 = gx[x] * colf[t];
+            // pass 0: K2 = g/M ; pass 1: K1 = g^2/M  (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
+            const T f = pass == 0 ? k2 * invM : (k2 * invM) * (k2 * invM) * a.Mreal;
+            buf[e].x *= f;
+            buf[e].y *= f;
+        }
+        __syncthreads();
+        cta_fft(buf, g.px, tc, tc, 1, true, twx, +1, a.err);
+        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+            const int x = e / tc, t = e - x * tc;
+            const int c = c0 + t;
+            if (c < ncol) sp[(size_t)x * ncol + c] = buf[e];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- Q and densities
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += sh[i];
+    return t;  // valid in thread 0
+}
+
+// partial sums of q^dagger(Nh) and q(Ns) (reduction_sum, GPU_kernels.h:58-90)
+template <typename T>
+__global__ void k_qsum(PropsArgs<T> a)
+{
+    __shared__ double sh[32];
+    const Geo &g = a.g;
+    const int slot = blockIdx.y;
+    const T *q2 = a.hist + hist_off<T>(g, slot, g.Nh, 1);
+    const T *q1 = a.hist + hist_off<T>(g, slot, g.Ns, 0);
+    double s2 = 0, s1 = 0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < g.M; r += gridDim.x * blockDim.x) {
+        s2 += (double)q2[r];
+        s1 += (double)q1[r];
+    }
+    double t2 = block_sum(s2, sh);
+    double t1 = block_sum(s1, sh);
+    if (threadIdx.x == 0) {
+        double *pp = a.partials + (size_t)slot * a.npart_stride;
+        pp[0 * gridDim.x + blockIdx.x] = t2;
+        pp[1 * gridDim.x + blockIdx.x] = t1;
+    }
+}
+
+// Q2, QC, lnQ and the ensemble weights (density.h:376-399); one block per slot
+template <typename T>
+__global__ void k_qfinal(PropsArgs<T> a, int nblk)
+{
+    const int slot = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    const double *pp = a.partials + (size_t)slot * a.npart_stride;
+    double Q2 = 0, QC = 0;
+    for (int i = 0; i < nblk; i++) Q2 += pp[i];
+    for (int i = 0; i < nblk; i++) QC += pp[nblk + i];
+    const double M = (double)a.g.M;
+    Q2 /= M;
+    QC /= M;
+    const int rep = a.slot_rep[slot];
+    double *rs = a.rs + (size_t)rep * kRsStride;
+    const double phic = a.phic, alpha = a.alpha;
+    double zB, zC, lnQ;
+    if (a.ens == 1) {
+        lnQ = phic * log(QC) + ((1.0 - phic) / alpha) * log(Q2);
+        zB = (1.0 - phic) / (Q2 * alpha);
+        zC = phic / QC;
+    } else {
+        zB = 1.0;
+        zC = phic;
+        lnQ = zB * Q2 + zC * QC;  // zA*Q1 = 0
+    }
+    rs[kRsQ2] = Q2;
+    rs[kRsQC] = QC;
+    rs[kRsLnQ] = lnQ;
+    rs[kRsZB] = zB;
+    rs[kRsZC] = zC;
+}
+
+__device__ __forceinline__ void kahan_add(double &sum, double &c, double term)
+{
+    const double y = term - c;
+    const double t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+}
+
+// Composite-Simpson densities (rA_rB_init_Ns_homo, rA_rB_mid_segments,
+// scale_concentrations, sumconcs2: GPU_kernels.h:92-139; loops density.h:402-430).
+// Weights 1, 4, 2, 4, ... restart at 4 for each block with no odd-count
+// correction, as in the reference.  Products are formed and summed in FP64
+// with Kahan compensation.  Also emits per-block partial sums of
+// rC, rA, rB, rhA, rhB and (chi*(phiA+phiB-1))^2.
+template <typename T>
+__global__ void k_density(PropsArgs<T> a)
+{
+    __shared__ double sh[32];
+    const Geo &g = a.g;
+    const int slot = blockIdx.y;
+    const int rep = a.slot_rep[slot];
+    const double *rs = a.rs + (size_t)rep * kRsStride;
+    const double zB = rs[kRsZB], zC = rs[kRsZC];
+    const double ds = 1.0 / g.Ns;
+    const int Ns = g.Ns, n1 = g.n1, n2 = g.n2, Nh = g.Nh;
+    const size_t M = g.M;
+    const T *h = a.hist + hist_off<T>(g, slot, 0, 0);
+    double *conc = a.conc + (size_t)rep * 4 * M;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < (int)M; r += gridDim.x * blockDim.x) {
+#define Q1(s) ((double)h[((size_t)(s) * 2 + 0) * M + r])
+#define Q2(s) ((double)h[((size_t)(s) * 2 + 1) * M + r])
+        double rhB = 2.0 * Q2(Nh), chB = 0;
+        const double q12 = Q1(n1) * Q2(n2);
+        double rCA = Q2(Ns) + q12, cA = 0;
+        double rCB = Q1(Ns) + q12, cB = 0;
+        int s, wt;
+        for (s = 1, wt = 4; s < Nh; s++, wt = 6 - wt) kahan_add(rhB, chB, wt * Q2(s) * Q2(Nh - s));
+        for (s = 1, wt = 4; s < n1; s++, wt = 6 - wt) kahan_add(rCA, cA, wt * Q1(s) * Q2(Ns - s));
+        for (s = n1 + 1, wt = 4; s < Ns; s++, wt = 6 - wt) kahan_add(rCB, cB, wt * Q1(s) * Q2(Ns - s));
+#undef Q1
+#undef Q2
+        const double rhA = 0.0;  // the A-homopolymer density is scaled by zA = 0
+        rhB = rhB * zB * ds / 3.0;
+        rCA = rCA * zC * ds / 3.0;
+        rCB = rCB * zC * ds / 3.0;
+        const double rA = rhA + rCA, rB = rhB + rCB;
+        conc[r] = rA;
+        conc[r + M] = rB;
+        conc[r + 2 * M] = rhA + rhB;
+        conc[r + 3 * M] = rCB;
+        const double dv = a.chi * (rB + rA - 1.0);
+        acc[0] += rCA + rCB;
+        acc[1] += rA;
+        acc[2] += rB;
+        acc[3] += rhA;
+        acc[4] += rhB;
+        acc[5] += dv * dv;
+    }
+    double *pp = a.partials + (size_t)slot * a.npart_stride;
+    for (int i = 0; i < 6; i++) {
+        double t = block_sum(acc[i], sh);
+        if (threadIdx.x == 0) pp[i * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// phis (density.h:433-454) and the W+ residual sum of solve_field0 (scft.cu:527-535)
+template <typename T>
+__global__ void k_dfinal(PropsArgs<T> a, int nblk)
+{
+    const int slot = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    const double *pp = a.partials + (size_t)slot * a.npart_stride;
+    const int rep = a.slot_rep[slot];
+    double *rs = a.rs + (size_t)rep * kRsStride;
+    double v[6];
+    for (int k = 0; k < 6; k++) {
+        double t = 0;
+        for (int i = 0; i < nblk; i++) t += pp[k * nblk + i];
+        v[k] = t;
+    }
+    const double M = (double)a.g.M;
+    for (int k = 0; k < 5; k++) rs[kRsPhis + k] = v[k] / M;
+    rs[kRsDev2] = v[5];
+}
+
+// ---------------------------------------------------------------- launchers
+// MT bounds the CTA size of the FFT kernels: 256 keeps the staged butterflies
+// in registers; 1024 serves slabs too large for 256 threads.
+template <typename T, int MT>
+int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
+{
+    const Geo &g = a.g;
+    dim3 gs(g.m0, 2, nslots), gp(g.ncol_tiles, 2, nslots);
+    k_prepare<T><<<dim3(L.ew_blocks, nslots), 256, 0, st>>>(a);
+    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, -1, 1);
+    for (int s = 0; s < g.Ns; s++) {
+        k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
+        k_mid<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
+        k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
+        k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+    }
+    k_qsum<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
+    k_qfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
+    k_density<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
+    k_dfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
+    return 4 * g.Ns + 6;
+}
+
+template <typename T>
+int launch_props(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
+{
+    return L.big ? launch_props_mt<T, 1024>(a, L, nslots, st) : launch_props_mt<T, 256>(a, L, nslots, st);
+}
+
+// one contour step s of slot 0 starting from the propagator store slice s
+template <typename T, int MT>
+int launch_single_step_mt(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st)
+{
+    const Geo &g = a.g;
+    dim3 gs(g.m0, 2, 1), gp(g.ncol_tiles, 2, 1);
+    k_prepare<T><<<dim3(L.ew_blocks, 1), 256, 0, st>>>(a);
+    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s - 1, 2);
+    k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
+    k_mid<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
+    k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
+    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+    return 6;
+}
+
+template <typename T>
+int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st)
+{
+    return L.big ? launch_single_step_mt<T, 1024>(a, L, s, st) : launch_single_step_mt<T, 256>(a, L, s, st);
+}
+
+template <typename T, int MT>
+int set_smem_mt(const PropsLaunch &L)
+{
+    cudaError_t e1 = cudaFuncSetAttribute(k_combine<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
+    cudaError_t e2 = cudaFuncSetAttribute(k_mid<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
+    cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : -1;
+}
+
+template <typename T>
+int set_props_smem(const PropsLaunch &L)
+{
+    return L.big ? set_smem_mt<T, 1024>(L) : set_smem_mt<T, 256>(L);
+}
+
+template int launch_props<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);
+template int launch_props<double>(const PropsArgs<double> &, const PropsLaunch &, int, cudaStream_t);
+template int launch_single_step<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);
+template int launch_single_step<double>(const PropsArgs<double> &, const PropsLaunch &, int, cudaStream_t);
+template int set_props_smem<float>(const PropsLaunch &);
+template int set_props_smem<double>(const PropsLaunch &);
+
+}  // namespace scft

@@ -1,0 +1,1086 @@
+// scft_ctx.cu -- host side of the C ABI (include/scft_b200.h): the device
+// context and the solver control flow of solve_field0 / solve_field / FreeE
+// (scft.cu:516-853) driving the sm_100a kernels.
+//
+// The heavy work (propagators, densities, residuals, spline, projection,
+// mixing) runs on the device; the host keeps only the per-replica scalars
+// the reference keeps (errors, mixing parameters, arc-length knots) and
+// evaluates them in FP64 in the reference's order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/scft_b200.h"
+#include "kernels.h"
+
+using namespace scft;
+
+namespace {
+
+constexpr int kRedBlocks = 148;  // reduction grid: one block per SM
+
+bool factor(int n, Plan1D &p)
+{
+    if (n < 1) return false;
+    p.n = n;
+    p.nst = 0;
+    int rem = n;
+    const int pref[] = {8, 4, 2, 3, 5, 7};
+    for (int R : pref)
+        while (rem % R == 0 && p.nst < kMaxStages) {
+            p.radix[p.nst++] = R;
+            rem /= R;
+        }
+    // a radix-2 stage after radix 8/4 stages is better merged: 8*2 -> 4*4
+    return rem == 1;
+}
+
+int slots_for(int R) { return 16 / R; }
+
+int threads_for(const Plan1D &p, int nlines)
+{
+    int need = 32;
+    for (int i = 0; i < p.nst; i++) {
+        const int R = p.radix[i];
+        const long nb = (long)nlines * (p.n / R);
+        const int t = (int)((nb + slots_for(R) - 1) / slots_for(R));
+        need = std::max(need, t);
+    }
+    return need;
+}
+
+int round32(int v) { return (v + 31) / 32 * 32; }
+
+}  // namespace
+
+struct scft_ctx {
+    scft_problem p;
+    Geo g;
+    int M, Mk, strn, nrep_alloc, nslots, prec;
+    double f;  // rounded A fraction
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PropsLaunch L;
+    std::string lasterr;
+
+    // device memory
+    double *W = nullptr, *conc = nullptr, *DEV = nullptr, *dWda = nullptr, *rs = nullptr;
+    double *partials = nullptr, *redout = nullptr;
+    int npart_stride = 0, nred_rows = 0;
+    int *rep_dev = nullptr, *err = nullptr;
+    void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
+         *kfac = nullptr;
+    SplineKnots *knots = nullptr;
+
+    // host state
+    std::vector<int> doiis;
+    std::vector<int> slot_of;   // replica -> slot of its last props (-1 unknown)
+    std::vector<double> rs_h;   // [rep][kRsStride]
+    std::vector<double> red_h;
+    scft_stats stats{};
+    bool timing_pending = false;
+
+    // solve_field loop state (scft.cu:561-590)
+    struct {
+        bool active = false;
+        int doii = -1, maxIter = 0, k = 0;
+        double errTol = 1e-3, lambda = 0.05, err = 1, errt = 1, FE = 0;
+        int dospring = 1, doredist = 0, doperp = 0;
+        std::vector<double> x, xref, alf, errs, errs3, FEs, FEs0, FEs1, phctot;
+        std::vector<int> steps;
+    } sf;
+};
+
+namespace {
+
+scft_status cuda_fail(scft_ctx *c, cudaError_t e, const char *what)
+{
+    c->lasterr = std::string(what) + ": " + cudaGetErrorString(e);
+    return SCFT_CUDA_ERROR;
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t _e = (call);                                   \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call);   \
+    } while (0)
+
+template <typename T>
+PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
+{
+    PropsArgs<T> a;
+    a.g = ctx->g;
+    a.slot_rep = slot_rep;
+    a.W = ctx->W;
+    a.conc = ctx->conc;
+    a.rs = ctx->rs;
+    a.etab = (T *)ctx->etab;
+    a.hist = (T *)ctx->hist;
+    a.spec = (cplx<T> *)ctx->spec;
+    a.pbuf = (T *)ctx->pbuf;
+    a.tw = (const cplx<T> *)ctx->tw;
+    a.kfac = (const T *)ctx->kfac;
+    a.partials = ctx->partials;
+    a.npart_stride = ctx->npart_stride;
+    a.invM = (T)(1.0 / ctx->M);
+    a.Mreal = (T)ctx->M;
+    a.chi = ctx->p.chi;
+    a.phic = ctx->p.phidb;
+    a.alpha = ctx->p.alpha;
+    a.ens = ctx->p.ens;
+    a.err = ctx->err;
+    return a;
+}
+
+FieldArgs field_args(scft_ctx *ctx, const int *rep_list)
+{
+    FieldArgs a;
+    a.M = ctx->M;
+    a.strn = ctx->strn;
+    a.rep_list = rep_list;
+    a.W = ctx->W;
+    a.conc = ctx->conc;
+    a.DEV = ctx->DEV;
+    a.dWda = ctx->dWda;
+    a.partials = ctx->partials;
+    a.chi = ctx->p.chi;
+    return a;
+}
+
+scft_status check_device_err(scft_ctx *ctx)
+{
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, ctx->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (e != 0) {
+        ctx->lasterr = "device kernel reported a launch-geometry error " + std::to_string(e);
+        return SCFT_CUDA_ERROR;
+    }
+    return SCFT_OK;
+}
+
+// uploads a replica list to the device (pageable copy: staged before return)
+scft_status upload_list(scft_ctx *ctx, const std::vector<int> &reps)
+{
+    CK(cudaMemcpyAsync(ctx->rep_dev, reps.data(), sizeof(int) * reps.size(), cudaMemcpyHostToDevice,
+                       ctx->st));
+    return SCFT_OK;
+}
+
+// density::props for a list of replicas; scalars land in ctx->rs_h
+scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
+{
+    if (reps.empty()) return SCFT_OK;
+    scft_status s = upload_list(ctx, reps);
+    if (s != SCFT_OK) return s;
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    int launches = 0;
+    for (size_t c0 = 0; c0 < reps.size(); c0 += ctx->nslots) {
+        const int nb = (int)std::min<size_t>(ctx->nslots, reps.size() - c0);
+        if (ctx->prec == SCFT_FP32)
+            launches += launch_props<float>(props_args<float>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+        else
+            launches += launch_props<double>(props_args<double>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+        for (int j = 0; j < nb; j++) {
+            for (auto &so : ctx->slot_of)
+                if (so == j) so = -1;
+            ctx->slot_of[reps[c0 + j]] = j;
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaMemcpyAsync(ctx->rs_h.data(), ctx->rs, sizeof(double) * ctx->rs_h.size(),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    s = check_device_err(ctx);
+    if (s != SCFT_OK) return s;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->stats.props_seconds += ms * 1e-3;
+    ctx->stats.props_calls += (long long)reps.size();
+    ctx->stats.contour_steps += (long long)reps.size() * ctx->g.Ns;
+    ctx->stats.kernel_launches += launches;
+    return SCFT_OK;
+}
+
+double rsv(const scft_ctx *ctx, int rep, int k) { return ctx->rs_h[(size_t)rep * kRsStride + k]; }
+
+// final reduction of `rows` partial rows into ctx->red_h
+scft_status reduce_rows(scft_ctx *ctx, int rows, int nblk)
+{
+    launch_reduce_final(ctx->partials, rows, nblk, ctx->redout, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->red_h.data(), ctx->redout, sizeof(double) * rows,
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
+// solve_field0 (scft.cu:516-554) over a set of replicas.  Replicas are
+// independent, so the batched form (all together, props per round) gives the
+// same per-replica results as the reference's one-after-another order.
+scft_status field0_set(scft_ctx *ctx, const std::vector<int> &set, int maxIter, double errTol,
+                       std::vector<int> &kout)
+{
+    struct St {
+        double lam = 0.05, err = 1.0, errt = 1.0;
+        int k = 1;
+    };
+    const double dlam1 = 1.09, dlam2 = 1.10;
+    std::vector<St> stt(ctx->nrep_alloc);
+    kout.assign(ctx->nrep_alloc, 0);
+    std::vector<std::vector<int>> groups;
+    if (ctx->p.batched)
+        groups.push_back(set);
+    else
+        for (int ii : set) groups.push_back({ii});
+    for (auto &grp : groups) {
+        std::vector<int> cur;
+        for (int ii : grp)
+            if (stt[ii].k < maxIter && stt[ii].err > errTol) cur.push_back(ii);
+        while (!cur.empty()) {
+            scft_status s = props_list(ctx, cur);
+            if (s != SCFT_OK) return s;
+            std::vector<double> lam(cur.size());
+            for (size_t j = 0; j < cur.size(); j++) {
+                St &q = stt[cur[j]];
+                q.err = std::pow(rsv(ctx, cur[j], kRsDev2) / ctx->M, 0.5);
+                if (!(q.err == q.err)) {
+                    ctx->lasterr = "solve_field0: residual is NaN for replica " + std::to_string(cur[j]);
+                    return SCFT_NAN_DETECTED;
+                }
+                lam[j] = q.lam;
+            }
+            s = upload_list(ctx, cur);
+            if (s != SCFT_OK) return s;
+            launch_mix0(field_args(ctx, ctx->rep_dev), (int)cur.size(), lam.data(), ctx->st);
+            ctx->stats.kernel_launches += 1;
+            CK(cudaGetLastError());
+            std::vector<int> nxt;
+            for (int ii : cur) {
+                St &q = stt[ii];
+                if (q.err < q.errt)
+                    q.lam = std::min(0.1, q.lam * dlam1);
+                else
+                    q.lam = std::max(0.005, q.lam / dlam2);
+                q.errt = q.err;
+                q.k++;
+                if (q.k < maxIter && q.err > errTol) nxt.push_back(ii);
+            }
+            cur.swap(nxt);
+        }
+    }
+    for (int ii : set) kout[ii] = stt[ii].k;
+    return SCFT_OK;
+}
+
+// EDist between consecutive replicas (scft.cu:351-355)
+scft_status edists(scft_ctx *ctx, std::vector<double> &del)
+{
+    const int n = ctx->strn - 1;
+    del.assign(std::max(n, 0), 0.0);
+    if (n <= 0) return SCFT_OK;
+    launch_edist(field_args(ctx, ctx->rep_dev), kRedBlocks, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    scft_status s = reduce_rows(ctx, n, kRedBlocks);
+    if (s != SCFT_OK) return s;
+    for (int i = 0; i < n; i++) del[i] = std::sqrt(ctx->red_h[i]);
+    return SCFT_OK;
+}
+
+// arc-length knots x (scft.cu:612-621, 725-736)
+scft_status arc_length(scft_ctx *ctx, std::vector<double> &x)
+{
+    std::vector<double> del;
+    scft_status s = edists(ctx, del);
+    if (s != SCFT_OK) return s;
+    const int strn = ctx->strn;
+    double Delsum = 0;
+    for (int ii = 0; ii < strn - 1; ii++) Delsum += del[ii];
+    for (int ii = 0; ii < strn - 1; ii++) del[ii] /= Delsum;
+    x.assign(strn, 0.0);
+    x[0] = 0;
+    x[strn - 1] = 1;
+    for (int ii = 1; ii < strn - 1; ii++) x[ii] = x[ii - 1] + del[ii - 1];
+    return SCFT_OK;
+}
+
+int interval(const std::vector<double> &x, double xx)
+{
+    int nm = 0;
+    for (size_t i = 0; i < x.size(); ++i) {
+        if (x[i] < xx)
+            nm = (int)i;
+        else
+            break;
+    }
+    return nm;
+}
+
+// knot-only parts of cubefit_chunk_g (GPU_kernels.h:253-267) and the interval
+// searches of eval_spline_*_chunk_g (GPU_kernels.h:292-297, 314-319)
+scft_status upload_knots(scft_ctx *ctx, const std::vector<double> &x, const std::vector<double> *xref,
+                         const int *doiis)
+{
+    SplineKnots K;
+    std::memset(&K, 0, sizeof(K));
+    const int strn = ctx->strn, n = strn - 1;
+    K.strn = strn;
+    for (int i = 0; i <= n - 1; ++i) K.h[i] = x[i + 1] - x[i];
+    K.l[0] = 1.0;
+    K.u[0] = 0.0;
+    for (int i = 1; i <= n - 1; ++i) {
+        K.l[i] = 2.0 * (x[i + 1] - x[i - 1]) - K.h[i - 1] * K.u[i - 1];
+        K.u[i] = K.h[i] / K.l[i];
+    }
+    if (n >= 0) K.l[n] = 1.0;
+    for (int ev = 0; ev < strn; ev++) {
+        K.nm_d[ev] = interval(x, x[ev]);
+        K.dx_d[ev] = x[ev] - x[K.nm_d[ev]];
+        if (xref) {
+            K.nm_v[ev] = interval(x, (*xref)[ev]);
+            K.dx_v[ev] = (*xref)[ev] - x[K.nm_v[ev]];
+        }
+        K.doiis[ev] = doiis[ev];
+    }
+    CK(cudaMemcpyAsync(ctx->knots, &K, sizeof(K), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));  // K lives on this stack frame
+    return SCFT_OK;
+}
+
+// FreeE, scft.cu:812-853 (single process: every replica is evaluated)
+scft_status free_energy(scft_ctx *ctx, double *FEout)
+{
+    auto &S = ctx->sf;
+    const int strn = ctx->strn;
+    std::vector<int> set;
+    for (int ii = 0; ii < strn; ii++)
+        if (ctx->doiis[ii] == 1 || ii == 0 || ii == strn - 1) set.push_back(ii);
+    std::vector<int> k0;
+    scft_status s = field0_set(ctx, set, 100, 1e-4, k0);
+    if (s != SCFT_OK) return s;
+    if (ctx->p.batched) {
+        s = props_list(ctx, set);
+        if (s != SCFT_OK) return s;
+    }
+    // plain mode: props of each replica right after its own W+ solve
+    std::vector<double> lnQ(strn, 0.0);
+    if (!ctx->p.batched) {
+        for (int ii : set) {
+            s = props_list(ctx, {ii});
+            if (s != SCFT_OK) return s;
+            lnQ[ii] = rsv(ctx, ii, kRsLnQ);
+        }
+    } else {
+        for (int ii : set) lnQ[ii] = rsv(ctx, ii, kRsLnQ);
+    }
+    s = upload_list(ctx, set);
+    if (s != SCFT_OK) return s;
+    launch_freee(field_args(ctx, ctx->rep_dev), (int)set.size(), ctx->f, kRedBlocks, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    s = reduce_rows(ctx, 2 * (int)set.size(), kRedBlocks);
+    if (s != SCFT_OK) return s;
+    for (size_t j = 0; j < set.size(); j++) {
+        const int ii = set[j];
+        S.FEs0[ii] = -lnQ[ii];
+        S.FEs1[ii] = ctx->red_h[2 * j];
+        S.phctot[ii] = ctx->red_h[2 * j + 1];
+        S.FEs[ii] = S.FEs0[ii] + S.FEs1[ii];
+    }
+    std::vector<double> del;
+    s = edists(ctx, del);
+    if (s != SCFT_OK) return s;
+    S.alf[0] = 0;
+    for (int ii = 1; ii < strn; ii++) S.alf[ii] = S.alf[ii - 1] + del[ii - 1];
+    double FE = 0;
+    for (int ii = 0; ii < strn; ii++) FE += S.FEs[ii];
+    if (FEout) *FEout = FE;
+    return SCFT_OK;
+}
+
+template <typename T>
+void upload_tables(scft_ctx *ctx, std::vector<unsigned char> &twb, std::vector<unsigned char> &kfb)
+{
+    const Geo &g = ctx->g;
+    const double PI = 3.14159265358979323846264338327950288;
+    const int ns[3] = {g.m0, g.m1, g.m2};
+    std::vector<cplx<T>> tw;
+    for (int a = 0; a < 3; a++)
+        for (int t = 0; t < ns[a]; t++) {
+            const double ang = 2.0 * PI * (double)t / (double)ns[a];
+            tw.push_back({(T)std::cos(ang), (T)(-std::sin(ang))});
+        }
+    // diffusion factor per axis: exp(-4 pi^2 k^2 ds / (12 D^2)) with k in
+    // [-(m-1)/2, m/2] (setup_k_sq, density.h:79-95); the last axis is halved
+    const double ds = 1.0 / g.Ns;
+    std::vector<T> kf;
+    for (int a = 0; a < 3; a++) {
+        const int m = ns[a];
+        const int cnt = a == 2 ? g.mk2 : m;
+        for (int K = 0; K < cnt; K++) {
+            const int k = (a == 2) ? K : (K <= m / 2 ? K : K - m);
+            const double A = (double)k * k / (ctx->p.D[a] * ctx->p.D[a]);
+            kf.push_back((T)std::exp(-4 * PI * PI * A * ds / 12));
+        }
+    }
+    twb.assign((unsigned char *)tw.data(), (unsigned char *)(tw.data() + tw.size()));
+    kfb.assign((unsigned char *)kf.data(), (unsigned char *)(kf.data() + kf.size()));
+}
+
+template <typename T>
+size_t elem() { return sizeof(T); }
+
+}  // namespace
+
+extern "C" {
+
+const char *scft_status_string(scft_status s)
+{
+    switch (s) {
+        case SCFT_OK: return "ok";
+        case SCFT_CUDA_ERROR: return "CUDA error";
+        case SCFT_NAN_DETECTED: return "NaN detected";
+        case SCFT_BAD_INPUT: return "bad input";
+        case SCFT_TIMEOUT: return "timeout";
+        case SCFT_OUT_OF_MEMORY: return "out of memory";
+        case SCFT_UNSUPPORTED: return "unsupported device";
+    }
+    return "unknown";
+}
+
+const char *scft_last_error(const scft_ctx *ctx) { return ctx ? ctx->lasterr.c_str() : "no context"; }
+
+void scft_destroy(scft_ctx *ctx)
+{
+    if (!ctx) return;
+    void *ptrs[] = {ctx->W, ctx->conc, ctx->DEV, ctx->dWda, ctx->rs, ctx->partials, ctx->redout,
+                    ctx->rep_dev, ctx->err, ctx->etab, ctx->hist, ctx->spec, ctx->pbuf, ctx->tw,
+                    ctx->kfac, ctx->knots};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+scft_status scft_create(const scft_problem *p, scft_ctx **out)
+{
+    if (!p || !out) return SCFT_BAD_INPUT;
+    *out = nullptr;
+    if (p->strn < 1 || p->strn > kMaxStrn || p->N < 1 || (p->ens != 1 && p->ens != 2) ||
+        (p->precision != SCFT_FP32 && p->precision != SCFT_FP64) || p->alpha < 0)
+        return SCFT_BAD_INPUT;
+    Geo g;
+    std::memset(&g, 0, sizeof(g));
+    g.m0 = p->m[0];
+    g.m1 = p->m[1];
+    g.m2 = p->m[2];
+    if (!factor(g.m0, g.px) || !factor(g.m1, g.py) || !factor(g.m2, g.pz)) return SCFT_BAD_INPUT;
+    g.mk2 = g.m2 / 2 + 1;
+    if (g.mk2 > 32 * kPairLanes) return SCFT_BAD_INPUT;
+    g.M = g.m0 * g.m1 * g.m2;
+    g.Mk = g.m0 * g.m1 * g.mk2;
+    g.npair = (g.m1 + 1) / 2;
+    g.slab_c = g.m1 * g.mk2 + g.m2 + 32;
+    const double f = std::round(p->N * p->f) / p->N;  // scft.cu:1008
+    g.Ns = p->N;
+    g.n1 = (int)std::round(g.Ns * f);  // density.h:346
+    g.n2 = g.Ns - g.n1;
+    g.Nh = (int)(p->alpha * g.Ns);
+    if (g.n1 < 0 || g.n1 > g.Ns || g.Nh > g.Ns) return SCFT_BAD_INPUT;
+
+    int dev = p->device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return SCFT_UNSUPPORTED;
+    if (prop.major != 10) return SCFT_UNSUPPORTED;
+    if (cudaSetDevice(dev) != cudaSuccess) return SCFT_UNSUPPORTED;
+
+    scft_ctx *ctx = new scft_ctx();
+    ctx->p = *p;
+    ctx->f = f;
+    ctx->prec = p->precision;
+    ctx->strn = p->strn;
+    ctx->M = g.M;
+    ctx->Mk = g.Mk;
+    ctx->nrep_alloc = p->strn + 1;  // + one scratch replica for scft_props_host
+    ctx->nslots = p->batched ? p->strn : 1;
+    const size_t T = p->precision == SCFT_FP32 ? 4 : 8;
+
+    // launch geometry
+    g.tc = T == 4 ? 32 : 16;
+    g.ncol_tiles = (g.m1 * g.mk2 + g.tc - 1) / g.tc;
+    PropsLaunch &L = ctx->L;
+    L.slab_threads = std::min(1024, std::max(256, round32(std::max(threads_for(g.pz, g.npair),
+                                                                      threads_for(g.py, g.mk2)))));
+    L.pencil_threads = std::min(1024, std::max(128, round32(threads_for(g.px, g.tc))));
+    L.big = (L.slab_threads > 256 || L.pencil_threads > 256) ? 1 : 0;
+    if (threads_for(g.pz, g.npair) > 1024 || threads_for(g.py, g.mk2) > 1024 ||
+        threads_for(g.px, g.tc) > 1024) {
+        delete ctx;
+        return SCFT_BAD_INPUT;
+    }
+    L.slab_smem = (int)((g.slab_c + g.m1 + g.m2) * 2 * T);
+    L.pencil_smem = (int)((g.tc * g.m0 + g.m0) * 2 * T + (g.tc + g.m0) * T);
+    L.ew_blocks = std::max(1, std::min(1024, (g.M + 255) / 256));
+    L.red_blocks = kRedBlocks;
+    if (L.slab_smem > (int)prop.sharedMemPerBlockOptin || L.pencil_smem > (int)prop.sharedMemPerBlockOptin) {
+        delete ctx;
+        return SCFT_BAD_INPUT;
+    }
+    ctx->g = g;
+    scft_status rc = SCFT_OK;
+    auto fail = [&](cudaError_t e, const char *what) {
+        ctx->lasterr = std::string(what) + ": " + cudaGetErrorString(e);
+        rc = (e == cudaErrorMemoryAllocation) ? SCFT_OUT_OF_MEMORY : SCFT_CUDA_ERROR;
+    };
+#define CKC(call)                      \
+    do {                               \
+        cudaError_t _e = (call);       \
+        if (_e != cudaSuccess) {       \
+            fail(_e, #call);           \
+            goto done;                 \
+        }                              \
+    } while (0)
+    {
+        const size_t M = g.M, R = ctx->nrep_alloc, S = ctx->nslots;
+        std::vector<unsigned char> twb, kfb;
+        if (T == 4)
+            upload_tables<float>(ctx, twb, kfb);
+        else
+            upload_tables<double>(ctx, twb, kfb);
+        ctx->npart_stride = 6 * kRedBlocks;
+        ctx->nred_rows = 2 * kMaxStrn + 8;
+        CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+        CKC(cudaEventCreate(&ctx->ev0));
+        CKC(cudaEventCreate(&ctx->ev1));
+        CKC(cudaMalloc(&ctx->W, sizeof(double) * 2 * M * R));
+        CKC(cudaMalloc(&ctx->conc, sizeof(double) * 4 * M * R));
+        CKC(cudaMalloc(&ctx->DEV, sizeof(double) * 2 * M * R));
+        CKC(cudaMalloc(&ctx->dWda, sizeof(double) * M * R));
+        CKC(cudaMalloc(&ctx->rs, sizeof(double) * kRsStride * R));
+        CKC(cudaMalloc(&ctx->partials,
+                       sizeof(double) * std::max<size_t>(ctx->npart_stride * S, (size_t)ctx->nred_rows * kRedBlocks)));
+        CKC(cudaMalloc(&ctx->redout, sizeof(double) * ctx->nred_rows));
+        CKC(cudaMalloc(&ctx->rep_dev, sizeof(int) * (R + 1)));
+        CKC(cudaMalloc(&ctx->err, sizeof(int)));
+        CKC(cudaMalloc(&ctx->etab, T * 2 * M * S));
+        CKC(cudaMalloc(&ctx->hist, T * 2 * M * (size_t)(g.Ns + 1) * S));
+        CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
+        CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
+        CKC(cudaMalloc(&ctx->tw, twb.size()));
+        CKC(cudaMalloc(&ctx->kfac, kfb.size()));
+        CKC(cudaMalloc(&ctx->knots, sizeof(SplineKnots)));
+        CKC(cudaMemcpy(ctx->tw, twb.data(), twb.size(), cudaMemcpyHostToDevice));
+        CKC(cudaMemcpy(ctx->kfac, kfb.data(), kfb.size(), cudaMemcpyHostToDevice));
+        CKC(cudaMemset(ctx->W, 0, sizeof(double) * 2 * M * R));
+        CKC(cudaMemset(ctx->conc, 0, sizeof(double) * 4 * M * R));
+        CKC(cudaMemset(ctx->DEV, 0, sizeof(double) * 2 * M * R));
+        CKC(cudaMemset(ctx->dWda, 0, sizeof(double) * M * R));
+        CKC(cudaMemset(ctx->rs, 0, sizeof(double) * kRsStride * R));
+        CKC(cudaMemset(ctx->err, 0, sizeof(int)));
+        if ((T == 4 ? set_props_smem<float>(L) : set_props_smem<double>(L)) != 0) {
+            ctx->lasterr = "cudaFuncSetAttribute(max dynamic shared memory) failed";
+            rc = SCFT_CUDA_ERROR;
+            goto done;
+        }
+        ctx->doiis.assign(ctx->strn, 1);  // one process owns every replica (scft.cu:952-975)
+        ctx->slot_of.assign(R, -1);
+        ctx->rs_h.assign(kRsStride * R, 0.0);
+        ctx->red_h.assign(ctx->nred_rows, 0.0);
+        auto &S_ = ctx->sf;
+        S_.x.assign(ctx->strn, 0.0);
+        S_.xref.assign(ctx->strn, 0.0);
+        S_.alf.assign(ctx->strn, 0.0);
+        S_.errs.assign(ctx->strn, 0.0);
+        S_.errs3.assign(ctx->strn, 0.0);
+        S_.FEs.assign(ctx->strn, 0.0);
+        S_.FEs0.assign(ctx->strn, 0.0);
+        S_.FEs1.assign(ctx->strn, 0.0);
+        S_.phctot.assign(ctx->strn, 0.0);
+        S_.steps.assign(ctx->strn, 0);
+    }
+done:
+#undef CKC
+    if (rc != SCFT_OK) {
+        std::string msg = ctx->lasterr;
+        scft_destroy(ctx);
+        fprintf(stderr, "scft_create: %s\n", msg.c_str());
+        return rc;
+    }
+    *out = ctx;
+    return SCFT_OK;
+}
+
+scft_status scft_set_fields(scft_ctx *ctx, int ii, const double *w2M)
+{
+    if (!ctx || !w2M || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    CK(cudaMemcpyAsync(ctx->W + (size_t)ii * 2 * ctx->M, w2M, sizeof(double) * 2 * ctx->M,
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
+scft_status scft_get_fields(const scft_ctx *cctx, int ii, double *w2M)
+{
+    scft_ctx *ctx = const_cast<scft_ctx *>(cctx);
+    if (!ctx || !w2M || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    CK(cudaMemcpyAsync(w2M, ctx->W + (size_t)ii * 2 * ctx->M, sizeof(double) * 2 * ctx->M,
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
+scft_status scft_get_conc(const scft_ctx *cctx, int ii, double *out4M, double *lnQ, double *phis)
+{
+    scft_ctx *ctx = const_cast<scft_ctx *>(cctx);
+    if (!ctx || ii < 0 || ii >= ctx->nrep_alloc) return SCFT_BAD_INPUT;
+    if (out4M) {
+        CK(cudaMemcpyAsync(out4M, ctx->conc + (size_t)ii * 4 * ctx->M, sizeof(double) * 4 * ctx->M,
+                           cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaMemcpyAsync(ctx->rs_h.data() + (size_t)ii * kRsStride, ctx->rs + (size_t)ii * kRsStride,
+                       sizeof(double) * kRsStride, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (lnQ) *lnQ = rsv(ctx, ii, kRsLnQ);
+    if (phis)
+        for (int k = 0; k < 5; k++) phis[k] = rsv(ctx, ii, kRsPhis + k);
+    return SCFT_OK;
+}
+
+scft_status scft_get_doiis(const scft_ctx *ctx, int *doiis)
+{
+    if (!ctx || !doiis) return SCFT_BAD_INPUT;
+    for (int i = 0; i < ctx->strn; i++) doiis[i] = ctx->doiis[i];
+    return SCFT_OK;
+}
+
+scft_status scft_props(scft_ctx *ctx, int ii)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    return props_list(ctx, {ii});
+}
+
+scft_status scft_props_host(scft_ctx *ctx, double *w, double *lnQ, int ii, int Ns, double alpha,
+                            double phic, double *phis, double f)
+{
+    (void)ii;
+    if (!ctx || !w) return SCFT_BAD_INPUT;
+    if (Ns != ctx->g.Ns || alpha != ctx->p.alpha || phic != ctx->p.phidb ||
+        (int)std::round(Ns * f) != ctx->g.n1) {
+        ctx->lasterr = "scft_props_host: Ns/alpha/phic/f differ from the context";
+        return SCFT_BAD_INPUT;
+    }
+    const int sc = ctx->strn;  // scratch replica
+    const size_t M = ctx->M;
+    CK(cudaMemcpyAsync(ctx->W + (size_t)sc * 2 * M, w, sizeof(double) * 2 * M, cudaMemcpyHostToDevice,
+                       ctx->st));
+    scft_status s = props_list(ctx, {sc});
+    if (s != SCFT_OK) return s;
+    CK(cudaMemcpyAsync(w + 2 * M, ctx->conc + (size_t)sc * 4 * M, sizeof(double) * 4 * M,
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (lnQ) *lnQ = rsv(ctx, sc, kRsLnQ);
+    if (phis)
+        for (int k = 0; k < 5; k++) phis[k] = rsv(ctx, sc, kRsPhis + k);
+    return SCFT_OK;
+}
+
+scft_status scft_do_step(scft_ctx *ctx, int ii, const double *in, double *out, int s)
+{
+    if (!ctx || !in || !out || ii < 0 || ii >= ctx->strn || s < 0 || s >= ctx->g.Ns)
+        return SCFT_BAD_INPUT;
+    const size_t M = ctx->M;
+    const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    const size_t slice = 2 * M;
+    std::vector<unsigned char> tmp(slice * T);
+    if (T == 4)
+        for (size_t i = 0; i < slice; i++) ((float *)tmp.data())[i] = (float)in[i];
+    else
+        std::memcpy(tmp.data(), in, slice * 8);
+    CK(cudaMemcpyAsync(ctx->rep_dev, &ii, sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    unsigned char *h0 = (unsigned char *)ctx->hist + (size_t)s * slice * T;
+    CK(cudaMemcpyAsync(h0, tmp.data(), slice * T, cudaMemcpyHostToDevice, ctx->st));
+    int nl;
+    if (T == 4)
+        nl = launch_single_step<float>(props_args<float>(ctx, ctx->rep_dev), ctx->L, s, ctx->st);
+    else
+        nl = launch_single_step<double>(props_args<double>(ctx, ctx->rep_dev), ctx->L, s, ctx->st);
+    ctx->stats.kernel_launches += nl;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(tmp.data(), h0 + slice * T, slice * T, cudaMemcpyDeviceToHost, ctx->st));
+    scft_status st = check_device_err(ctx);
+    if (st != SCFT_OK) return st;
+    for (auto &so : ctx->slot_of)
+        if (so == 0) so = -1;
+    if (T == 4)
+        for (size_t i = 0; i < slice; i++) out[i] = ((float *)tmp.data())[i];
+    else
+        std::memcpy(out, tmp.data(), slice * 8);
+    return SCFT_OK;
+}
+
+scft_status scft_get_propagator(const scft_ctx *cctx, int ii, int which, int s, double *outM)
+{
+    scft_ctx *ctx = const_cast<scft_ctx *>(cctx);
+    if (!ctx || !outM || ii < 0 || ii >= ctx->nrep_alloc || s < 0 || s > ctx->g.Ns) return SCFT_BAD_INPUT;
+    const int slot = ctx->slot_of[ii];
+    if (slot < 0) {
+        ctx->lasterr = "propagators of this replica are no longer resident";
+        return SCFT_BAD_INPUT;
+    }
+    const size_t M = ctx->M, T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    const size_t off = (((size_t)slot * (ctx->g.Ns + 1) + s) * 2 + (which ? 1 : 0)) * M;
+    std::vector<unsigned char> tmp(M * T);
+    CK(cudaMemcpyAsync(tmp.data(), (unsigned char *)ctx->hist + off * T, M * T, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (T == 4)
+        for (size_t i = 0; i < M; i++) outM[i] = ((float *)tmp.data())[i];
+    else
+        std::memcpy(outM, tmp.data(), M * 8);
+    return SCFT_OK;
+}
+
+scft_status scft_solve_field0(scft_ctx *ctx, int ii, int maxIter, double errTol, int *k_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    std::vector<int> k;
+    scft_status s = field0_set(ctx, {ii}, maxIter, errTol, k);
+    if (k_out) *k_out = k.empty() ? 0 : k[ii];
+    return s;
+}
+
+scft_status scft_solve_field0_all(scft_ctx *ctx, int maxIter, double errTol, int *k_out)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    std::vector<int> set;
+    for (int ii = 0; ii < ctx->strn; ii++)
+        if (ctx->doiis[ii] == 1) set.push_back(ii);
+    std::vector<int> k;
+    scft_status s = field0_set(ctx, set, maxIter, errTol, k);
+    if (k_out)
+        for (int ii = 0; ii < ctx->strn; ii++) k_out[ii] = k.empty() ? 0 : k[ii];
+    return s;
+}
+
+scft_status scft_string_begin(scft_ctx *ctx, int doii, int maxIter, double errTol)
+{
+    if (!ctx || doii < -1 || doii >= ctx->strn) return SCFT_BAD_INPUT;
+    auto &S = ctx->sf;
+    S.active = true;
+    S.doii = doii;
+    S.maxIter = maxIter;
+    S.errTol = errTol;
+    S.k = 0;
+    S.lambda = 0.05;
+    S.err = 1;
+    S.errt = 1;
+    S.dospring = 1;
+    S.doredist = 0;
+    S.doperp = 0;
+    if (doii > -1 || ctx->p.dostring != 1) S.dospring = S.doredist = S.doperp = 0;
+    if (ctx->p.fix[0] == 1) ctx->doiis[0] = 0;  // scft.cu:587-588
+    if (ctx->p.fix[1] == 1) ctx->doiis[ctx->strn - 1] = 0;
+    std::fill(S.steps.begin(), S.steps.end(), 0);
+    return SCFT_OK;
+}
+
+// one k-pass of the solve_field loop, scft.cu:592-806
+scft_status scft_string_step(scft_ctx *ctx, scft_iter_report *rep, double *errs_out,
+                             double *errs3_out, int *done)
+{
+    if (!ctx || !ctx->sf.active) return SCFT_BAD_INPUT;
+    auto &S = ctx->sf;
+    const int strn = ctx->strn, doii = S.doii;
+    const size_t M = ctx->M;
+    const double eps = 0.5;
+    const int skip = 50;
+    scft_status s;
+    if (!(S.k < S.maxIter && S.err > S.errTol)) {
+        if (done) *done = 1;
+        return SCFT_OK;
+    }
+    const int k = S.k;
+    if (k >= ctx->p.springsteps && doii == -1 && ctx->p.dostring == 1) {
+        S.dospring = 0;
+        S.doredist = 1;
+        S.doperp = 1;
+    }
+    CK(cudaMemsetAsync(ctx->DEV, 0, sizeof(double) * 2 * M * strn, ctx->st));
+    std::vector<int> set;
+    for (int ii = 0; ii < strn; ii++) {
+        S.steps[ii] = 0;
+        if ((ctx->doiis[ii] == 1 && doii == -1) || doii == ii) set.push_back(ii);
+    }
+    for (int ii : set) S.steps[ii]++;
+    std::vector<int> k0;
+    s = field0_set(ctx, set, 20, S.errTol, k0);
+    if (s != SCFT_OK) return s;
+    for (int ii : set) S.steps[ii] += k0[ii];
+    if (ctx->p.batched) {
+        s = props_list(ctx, set);
+        if (s != SCFT_OK) return s;
+    } else {
+        for (int ii : set) {
+            s = props_list(ctx, {ii});
+            if (s != SCFT_OK) return s;
+        }
+    }
+    // residuals DEV (scft.cu:604-608)
+    std::vector<double> sum2(strn, 0.0), summ(strn, 0.0);
+    if (!set.empty()) {
+        s = upload_list(ctx, set);
+        if (s != SCFT_OK) return s;
+        launch_dev(field_args(ctx, ctx->rep_dev), (int)set.size(), kRedBlocks, S.dospring, eps, ctx->st);
+        ctx->stats.kernel_launches += 1;
+        s = reduce_rows(ctx, 2 * (int)set.size(), kRedBlocks);
+        if (s != SCFT_OK) return s;
+        for (size_t j = 0; j < set.size(); j++) {
+            sum2[set[j]] = ctx->red_h[2 * j];
+            summ[set[j]] = ctx->red_h[2 * j + 1];
+        }
+    }
+    if (doii == -1) {
+        s = arc_length(ctx, S.x);
+        if (s != SCFT_OK) return s;
+        for (int ii = 0; ii < strn; ii++) S.xref[ii] = (1.0 * ii) / (strn - 1.0);
+        for (int ii = 0; ii < strn; ii++) S.errs[ii] = std::pow(sum2[ii] / (2 * (double)M), 0.5);
+    } else {
+        for (int ii = 0; ii < strn; ii++) S.errs[ii] = 0;
+        S.errs[doii] = std::pow(sum2[doii] / (2 * (double)M), 0.5);
+    }
+    if (S.doperp == 1) {
+        // spline derivative along the string and projection (scft.cu:641-683)
+        s = upload_knots(ctx, S.x, nullptr, ctx->doiis.data());
+        if (s != SCFT_OK) return s;
+        launch_spline_deriv(field_args(ctx, ctx->rep_dev), ctx->knots, 4 * kRedBlocks, ctx->st);
+        ctx->stats.kernel_launches += 1;
+        std::vector<int> dset;
+        for (int ii = 0; ii < strn; ii++)
+            if (ctx->doiis[ii] == 1) dset.push_back(ii);
+        std::vector<double> normDER(strn, 0.0), normDEV(strn, 0.0), dotWs(strn, 0.0);
+        if (!dset.empty()) {
+            s = upload_list(ctx, dset);
+            if (s != SCFT_OK) return s;
+            launch_dots(field_args(ctx, ctx->rep_dev), (int)dset.size(), kRedBlocks, ctx->st);
+            ctx->stats.kernel_launches += 1;
+            s = reduce_rows(ctx, 2 * (int)dset.size(), kRedBlocks);
+            if (s != SCFT_OK) return s;
+            for (size_t j = 0; j < dset.size(); j++) {
+                const int ii = dset[j];
+                normDER[ii] = std::sqrt(ctx->red_h[2 * j]);
+                normDEV[ii] = std::sqrt(summ[ii]);
+                dotWs[ii] = ctx->red_h[2 * j + 1] / (normDEV[ii] * normDER[ii]);
+            }
+        }
+        for (int ii = 0; ii < strn; ii++) S.errs3[ii] = 0;
+        std::vector<int> pset;
+        std::vector<double> coef, ndev;
+        for (int ii = 1; ii < strn - 1; ii++) {
+            if (ctx->doiis[ii] == 1 && normDER[ii] > 0 && normDEV[ii] > 0) {
+                pset.push_back(ii);
+                coef.push_back(dotWs[ii] / normDER[ii]);
+                ndev.push_back(normDEV[ii]);
+            } else if (ctx->doiis[ii] == 1) {
+                fprintf(stderr, "Fatal error occurred (0)... %d %d %lf %lf\n", k, ii, normDER[ii],
+                        normDEV[ii]);
+            }
+        }
+        if (!pset.empty()) {
+            s = upload_list(ctx, pset);
+            if (s != SCFT_OK) return s;
+            launch_perp(field_args(ctx, ctx->rep_dev), (int)pset.size(), coef.data(), ndev.data(),
+                        kRedBlocks, ctx->st);
+            ctx->stats.kernel_launches += 1;
+            s = reduce_rows(ctx, (int)pset.size(), kRedBlocks);
+            if (s != SCFT_OK) return s;
+            for (size_t j = 0; j < pset.size(); j++)
+                S.errs3[pset[j]] = std::pow(ctx->red_h[j] / (2 * (double)M), 0.5);
+        }
+    } else {
+        for (int ii = 0; ii < strn; ii++) S.errs3[ii] = S.errs[ii];
+    }
+    S.errs3[0] = S.errs[0];
+    S.errs3[strn - 1] = S.errs[strn - 1];
+    // simple mixing with fixed mixing parameter (scft.cu:691-693)
+    launch_mix(field_args(ctx, ctx->rep_dev), S.lambda, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    CK(cudaGetLastError());
+    double stepav = 0;
+    for (int ii = 0; ii < strn; ii++) stepav += S.steps[ii];
+    stepav /= strn;
+    double fitup = 0;
+    std::vector<double> xnew = S.x;
+    if (doii == -1) {
+        s = arc_length(ctx, xnew);
+        if (s != SCFT_OK) return s;
+        for (int ii = 0; ii < strn; ii++) S.alf[ii] = xnew[ii];
+        for (int ii = 1; ii < strn - 1; ii++) fitup += std::pow(xnew[ii] - S.xref[ii], 2.0);
+        fitup /= strn - 2.0;
+        fitup = std::sqrt(fitup);
+        fitup /= strn - 1.0;
+        S.x = xnew;
+    }
+    if (S.doredist == 1) {
+        // equal-arc redistribution (scft.cu:745-757)
+        s = upload_knots(ctx, S.x, &S.xref, ctx->doiis.data());
+        if (s != SCFT_OK) return s;
+        launch_redist(field_args(ctx, ctx->rep_dev), ctx->knots, S.lambda, 4 * kRedBlocks, ctx->st);
+        ctx->stats.kernel_launches += 1;
+        CK(cudaGetLastError());
+    }
+    double errtot = 0;
+    for (int ii = 0; ii < strn; ii++) errtot += S.errs3[ii] * S.errs3[ii] / strn;
+    errtot = std::sqrt(errtot);
+    int did_fe = 0;
+    if (k % skip == 0 || k == S.maxIter - 1 || !(S.err > S.errTol)) {
+        s = free_energy(ctx, &S.FE);
+        if (s != SCFT_OK) return s;
+        did_fe = 1;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    if (rep) {
+        rep->k = k;
+        rep->lambda = S.lambda;
+        rep->errtot = errtot;
+        rep->fitup = fitup;
+        rep->stepav = stepav;
+        rep->did_freee = did_fe;
+        rep->FE = did_fe ? S.FE : 0.0;
+    }
+    if (errs_out) std::memcpy(errs_out, S.errs.data(), sizeof(double) * strn);
+    if (errs3_out) std::memcpy(errs3_out, S.errs3.data(), sizeof(double) * strn);
+    // mixing-parameter update (scft.cu:793-798): err stays 1, so lambda stays 0.05
+    if (S.err < S.errt)
+        S.lambda = std::min(0.2, S.lambda * 1.015);
+    else
+        S.lambda = std::max(0.05, S.lambda / 1.016);
+    S.errt = S.err;
+    S.k++;
+    if (done) *done = (S.k < S.maxIter && S.err > S.errTol) ? 0 : 1;
+    return SCFT_OK;
+}
+
+scft_status scft_string_end(scft_ctx *ctx, int *k_out)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    if (k_out) *k_out = ctx->sf.k;
+    ctx->sf.active = false;
+    return SCFT_OK;
+}
+
+scft_status scft_solve_field(scft_ctx *ctx, int doii, int maxIter, double errTol,
+                             scft_iter_report *reports, double *errs, double *errs3, int *k_out)
+{
+    scft_status s = scft_string_begin(ctx, doii, maxIter, errTol);
+    if (s != SCFT_OK) return s;
+    int done = 0;
+    while (!done) {
+        const int k = ctx->sf.k;
+        if (!(k < maxIter && ctx->sf.err > errTol)) break;
+        s = scft_string_step(ctx, reports ? reports + k : nullptr,
+                             errs ? errs + (size_t)k * ctx->strn : nullptr,
+                             errs3 ? errs3 + (size_t)k * ctx->strn : nullptr, &done);
+        if (s != SCFT_OK) return s;
+    }
+    return scft_string_end(ctx, k_out);
+}
+
+scft_status scft_free_energy(scft_ctx *ctx, double *FE, double *FEs, double *FEs0, double *FEs1,
+                             double *phctot, double *alf)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    double fe = 0;
+    scft_status s = free_energy(ctx, &fe);
+    if (s != SCFT_OK) return s;
+    const size_t n = sizeof(double) * ctx->strn;
+    if (FE) *FE = fe;
+    if (FEs) std::memcpy(FEs, ctx->sf.FEs.data(), n);
+    if (FEs0) std::memcpy(FEs0, ctx->sf.FEs0.data(), n);
+    if (FEs1) std::memcpy(FEs1, ctx->sf.FEs1.data(), n);
+    if (phctot) std::memcpy(phctot, ctx->sf.phctot.data(), n);
+    if (alf) std::memcpy(alf, ctx->sf.alf.data(), n);
+    return SCFT_OK;
+}
+
+// density::splineDerivsChunked with host arrays (density.h:491-508).  Uses the
+// device W- storage of the context as staging (replicas' fields are restored).
+static scft_status spline_host(scft_ctx *ctx, const double *x, const double *xref,
+                               const double *const *ww, double *const *out, double *const *wio,
+                               int r0, int n, const int *doiis, double lambda)
+{
+    if (!ctx || !x || n < 0 || r0 < 0 || r0 + n > ctx->M) return SCFT_BAD_INPUT;
+    const int strn = ctx->strn;
+    const size_t M = ctx->M;
+    // save W-, stage the chunk at the start of each replica's W- row
+    std::vector<double> saved(2 * M * strn);
+    CK(cudaMemcpyAsync(saved.data(), ctx->W, sizeof(double) * 2 * M * strn, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::vector<double> stage(saved);
+    for (int ii = 0; ii < strn; ii++) {
+        const double *src = ww ? ww[ii] : wio[ii];
+        std::memcpy(stage.data() + (size_t)ii * 2 * M, src + r0, sizeof(double) * n);
+    }
+    CK(cudaMemcpyAsync(ctx->W, stage.data(), sizeof(double) * 2 * M * strn, cudaMemcpyHostToDevice, ctx->st));
+    std::vector<double> xv(x, x + strn), xr;
+    if (xref) xr.assign(xref, xref + strn);
+    scft_status s = upload_knots(ctx, xv, xref ? &xr : nullptr, doiis);
+    if (s != SCFT_OK) return s;
+    FieldArgs a = field_args(ctx, ctx->rep_dev);
+    a.M = (int)M;
+    if (out) {
+        launch_spline_deriv(a, ctx->knots, 4 * kRedBlocks, ctx->st);
+        std::vector<double> d(M * strn);
+        CK(cudaMemcpyAsync(d.data(), ctx->dWda, sizeof(double) * M * strn, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int ii = 0; ii < strn; ii++)
+            if (doiis[ii] == 1) std::memcpy(out[ii] + r0, d.data() + (size_t)ii * M, sizeof(double) * n);
+    } else {
+        launch_redist(a, ctx->knots, lambda, 4 * kRedBlocks, ctx->st);
+        std::vector<double> w(2 * M * strn);
+        CK(cudaMemcpyAsync(w.data(), ctx->W, sizeof(double) * 2 * M * strn, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int ii = 1; ii < strn - 1; ii++)
+            if (doiis[ii] == 1) std::memcpy(wio[ii] + r0, w.data() + (size_t)ii * 2 * M, sizeof(double) * n);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->W, saved.data(), sizeof(double) * 2 * M * strn, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
+scft_status scft_spline_derivs(scft_ctx *ctx, const double *x, const double *const *ww, int r0, int n,
+                               const int *doiis, double *const *out)
+{
+    if (!ww || !out || !doiis) return SCFT_BAD_INPUT;
+    return spline_host(ctx, x, nullptr, ww, out, nullptr, r0, n, doiis, 0.0);
+}
+
+scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xref, double *const *ww,
+                               int r0, int n, const int *doiis, double lambda)
+{
+    if (!ww || !xref || !doiis) return SCFT_BAD_INPUT;
+    return spline_host(ctx, x, xref, nullptr, nullptr, ww, r0, n, doiis, lambda);
+}
+
+scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st)
+{
+    if (!ctx || !st) return SCFT_BAD_INPUT;
+    *st = ctx->stats;
+    return SCFT_OK;
+}
+
+scft_status scft_reset_stats(scft_ctx *ctx)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    ctx->stats = scft_stats{};
+    return SCFT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,315 @@
+#!/usr/bin/env python3
+"""Benchmark: string iterations per second of the SCFT string method.
+
+Workload: the 16-replica 64^3 string (N=128, chiN=14, f=0.45, phidb=0.85,
+D=5, fixed ends; ens=2, the reference default), seeded synthetic fields
+(scft_string_b200.configs.STRING_64).  One step = one iteration of the
+reference's solve_field loop (scft.cu:592-806): inner W+ relaxation and props
+of every replica, residuals, spline tangent projection, mixing and equal-arc
+redistribution.  Each rank runs its own copy of the string (replicas only, no
+collective on the data path); value = steps of all ranks / max-rank device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp32|fp64] [--plain]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "String iters/s @ RMS err≤1e-5, batched fused FP32 vs plain FP64 on 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--plain", action="store_true", help="one replica at a time")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 8:
+                    rows.append(t)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = sorted(float(r[0]) for r in rows if r[0].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per replica contour step from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "step_traffic.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("dram_bytes_per_replica_step"):
+                    return float(line.split()[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(cfg, props_per_iter):
+    """The FP64 oracle (the reference algorithm restated in C, OpenMP over
+    grid points) timed on the host cores: a bounded sample of props calls of
+    one replica of the workload."""
+    import numpy as np
+
+    import oracle as O
+    from scft_string_b200.configs import fields
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    wm, wp = fields(cfg)
+    M = wm.shape[1]
+    d = O.Density(cfg["m"], cfg["D"], cfg["N"])
+    w = np.zeros(6 * M)
+    w[:M], w[M:2 * M] = wm[1], wp[1]
+    f = round(cfg["N"] * cfg["f"]) / cfg["N"]
+    t0 = time.time()
+    n = 0
+    while n < 3 or (time.time() - t0 < 10 and n < 20):
+        d.props(w, cfg["N"], cfg.get("alpha", 0.1), cfg["phidb"], f, cfg["ens"])
+        n += 1
+    tp = (time.time() - t0) / n
+    return {"value": 1.0 / (props_per_iter * cfg["strn"] * tp), "unit": "string iters/s",
+            "cores": cores, "kind": "port",
+            "sample": f"{n} props calls of one replica (64^3, N=128, FP64, {cores} threads), "
+                      f"{tp:.3f} s each; rate = 1/(props per iteration x replicas x that time) with "
+                      f"{props_per_iter:.2f} props per replica per iteration as measured on the GPU",
+            "contour_steps_per_s": cfg["N"] / tp}
+
+
+def run_ours(a, cfg, rank, world, dev):
+    import numpy as np
+    import torch
+
+    import scft_string_b200 as S
+    from scft_string_b200.configs import fields
+
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", dev))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    wm, wp = fields(cfg)
+    ctx = S.StringSolver(cfg, precision=a.precision, batched=not a.plain, device=dev)
+    for ii in range(cfg["strn"]):
+        ctx.set_fields(ii, wm[ii], wp[ii])
+    ctx.solve_field0_all(5000, 1e-4)           # prelude, scft.cu:1105
+    nsterp = 4000                              # scft.cu:1102
+    ctx.string_begin(nsterp, 1e-3)
+    for _ in range(a.warmup):
+        ctx.string_step()
+    # ---- timed: K iterations with device-resident fields
+    barrier()
+    clk = Clocks(dev) if rank == 0 else None
+    ctx.reset_stats()
+    ctx.timer_mark(0)
+    reps = [ctx.string_step() for _ in range(a.steps)]
+    ctx.timer_mark(1)
+    ms = ctx.timer_elapsed_ms(0, 1)
+    barrier()
+    clocks = clk.stop() if clk else None
+    st = ctx.stats()
+    ms_max = max_over_ranks(ms)
+    # ---- e2e: host-owned fields (pinned), H2D + step + D2H every iteration
+    M = ctx.M
+    host = torch.empty((cfg["strn"], 2 * M), dtype=torch.float64, pin_memory=True).numpy()
+    for ii in range(cfg["strn"]):
+        host[ii] = ctx.get_fields(ii)
+    barrier()
+    ctx.timer_mark(2)
+    for _ in range(a.steps):
+        for ii in range(cfg["strn"]):
+            ctx.set_fields(ii, host[ii][:M], host[ii][M:])
+        ctx.string_step()
+        for ii in range(cfg["strn"]):
+            host[ii][:] = ctx.get_fields(ii)
+    ctx.timer_mark(3)
+    e2e_ms = max_over_ranks(ctx.timer_elapsed_ms(2, 3))
+    barrier()
+    out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M)
+    # ---- plain FP64 path on the same state, same first iterations
+    if rank == 0 and world == 1 and not a.no_fp64 and a.precision == "fp32":
+        k2 = min(2, a.steps)
+        ctx64 = S.StringSolver(cfg, precision="fp64", batched=False, device=dev)
+        ctx32 = S.StringSolver(cfg, precision="fp32", batched=True, device=dev)
+        for ii in range(cfg["strn"]):
+            w = host[ii]
+            ctx64.set_fields(ii, w[:M], w[M:])
+            ctx32.set_fields(ii, w[:M], w[M:])
+        res = {}
+        for name, c in (("fp64_plain", ctx64), ("fp32_batched", ctx32)):
+            c.string_begin(nsterp, 1e-3)
+            c.string_step()  # k = 0 runs FreeE; time the following iterations
+            c.reset_stats()
+            c.timer_mark(0)
+            for _ in range(k2):
+                c.string_step()
+            c.timer_mark(1)
+            t = c.timer_elapsed_ms(0, 1)
+            s2 = c.stats()
+            res[name] = dict(iters_per_s=k2 / (t / 1e3),
+                             contour_steps_per_s=s2["contour_steps"] / s2["props_seconds"],
+                             iters=k2)
+            c.close()
+        out["fp64_cmp"] = res
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return out
+
+
+def main():
+    a = parse()
+    rank, world, dev = dist_env()
+    from scft_string_b200.configs import STRING_64
+    cfg = dict(STRING_64)
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle.refrun import time_iterations
+        r = time_iterations(cfg, a.warmup, a.steps)
+        if "unavailable" in r:
+            print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+            return 0
+        v = r["iters_per_s"]
+        line = {"metric": METRIC, "value": v, "unit": "string iters/s", "n_gpus": 1,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded fields, scft_string_b200.configs)",
+                "config": {"workload": cfg["name"], "replicas": cfg["strn"], "grid": list(cfg["m"]),
+                           "N": cfg["N"], "ens": cfg["ens"],
+                           "program": "reference scft.cu built for sm_100a (oracle/build_ref.sh), "
+                                      "single rank owning every replica"},
+                "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "string iters/s", "cores": 1,
+                                 "kind": "reference",
+                                 "sample": "reference program on the GPU (its only implementation "
+                                           "is CUDA); host thread count 1"},
+                "e2e": {"value": v, "unit": "string iters/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    r = run_ours(a, cfg, rank, world, dev)
+    if rank != 0:
+        return 0
+    st, reps = r["stats"], r["reps"]
+    M = r["M"]
+    b = 4 if a.precision == "fp32" else 8
+    step_bytes = 8 * M * b                              # algorithmic bytes per replica contour step
+    achieved = step_bytes * st["contour_steps"] / st["props_seconds"] / 1e9
+    peak, peak_kind = peaks()
+    traffic = profiled_traffic()
+    value = world * a.steps / (r["ms"] / 1e3)
+    props_per_iter = st["props_calls"] / (a.steps * cfg["strn"])
+    import math
+    flops = 30.0 * M * math.log2(M) * st["contour_steps"] / st["props_seconds"] / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "string iters/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["ms"] / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == "fp32" else "f64",
+        "data": "synthetic (seeded fields, scft_string_b200.configs)",
+        "config": {"workload": cfg["name"], "replicas": cfg["strn"], "grid": list(cfg["m"]),
+                   "N": cfg["N"], "ens": cfg["ens"], "precision": a.precision,
+                   "batched": not a.plain, "parallelism": f"replicas-only x{world}",
+                   "window": f"iterations k={a.warmup}..{a.warmup + a.steps - 1} after the W+ prelude",
+                   "l2": "inputs larger than L2 (propagator store "
+                         f"{cfg['strn'] * (cfg['N'] + 1) * 2 * M * b / 1e9:.1f} GB per props round)"},
+        "errtot_last": reps[-1]["errtot"], "props_per_replica_iter": props_per_iter,
+        "contour_steps_per_s": st["contour_steps"] / st["props_seconds"],
+        "gpu_launches": st["kernel_launches"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None if traffic is None else traffic * 1.0,
+                     "unit_of_work": "replica contour step (q and q^dagger advanced by ds)",
+                     "algorithmic_bytes_per_unit": step_bytes,
+                     "fp32_tflops": flops},
+        "e2e": {"value": world * a.steps / (r["e2e_ms"] / 1e3), "unit": "string iters/s",
+                "h2d_bytes_per_step": cfg["strn"] * 2 * M * 8,
+                "d2h_bytes_per_step": cfg["strn"] * 2 * M * 8},
+        "clocks": r["clocks"],
+    }
+    if "fp64_cmp" in r:
+        c = r["fp64_cmp"]
+        line["fp64_plain_cmp"] = c
+        line["speedup_vs_fp64_plain"] = c["fp32_batched"]["iters_per_s"] / c["fp64_plain"]["iters_per_s"]
+    if world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(cfg, props_per_iter)
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -134,6 +134,11 @@ scft_status scft_string_end(scft_ctx *ctx, int *k_out);
 scft_status scft_free_energy(scft_ctx *ctx, double *FE, double *FEs, double *FEs0, double *FEs1,
                              double *phctot, double *alf);
 
+/* Results of the last FreeE evaluation (inside scft_solve_field every 50
+ * iterations, or scft_free_energy) without recomputing; any may be NULL. */
+scft_status scft_last_free_energy(const scft_ctx *ctx, double *FE, double *FEs, double *FEs0,
+                                  double *FEs1, double *phctot, double *alf);
+
 /* ---- string spline services (host pointers) --------------------------- */
 /* density::splineDerivsChunked (density.h:491-508): ww[ii] -> W- of replica
  * ii; out[ii][r0..r0+n) = dW-/dalpha at knot x[ii] for doiis[ii] == 1. */
@@ -145,6 +150,10 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
                                double *const *ww, int r0, int n, const int *doiis, double lambda);
 
 /* ---- statistics ------------------------------------------------------- */
+/* Records CUDA event `slot` (0..3) on the context's stream; elapsed device
+ * time between two recorded slots (waits for the later one). */
+scft_status scft_timer_mark(scft_ctx *ctx, int slot);
+scft_status scft_timer_elapsed(scft_ctx *ctx, int slot_a, int slot_b, double *ms);
 scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
 scft_status scft_reset_stats(scft_ctx *ctx);
 

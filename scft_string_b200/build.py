@@ -1,0 +1,46 @@
+"""Builds the sm_100a shared library ``libscft_b200.so`` and the drop-in
+executable ``scft_b200`` in-tree with nvcc (no JIT cache, no CPU fallback)."""
+from __future__ import annotations
+
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libscft_b200.so")
+EXE = os.path.join(HERE, "scft_b200")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.h"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "scft_b200.h"))
+    if force or _stale(LIB, deps):
+        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+               "-o", LIB] + [os.path.join(CSRC, f) for f in CU_SOURCES]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    main = os.path.join(CSRC, "scft_main.cpp")
+    if os.path.exists(main) and (force or _stale(EXE, [main, LIB])):
+        cmd = [NVCC, "-O2", "-std=c++17", *ARCH, "-o", EXE, main, "-L" + HERE, "-lscft_b200",
+               "-Xlinker", "-rpath=$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose=True)

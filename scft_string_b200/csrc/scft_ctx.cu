@@ -65,6 +65,7 @@ struct scft_ctx {
     double f;  // rounded A fraction
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
     PropsLaunch L;
     std::string lasterr;
 
@@ -463,6 +464,8 @@ void scft_destroy(scft_ctx *ctx)
                     ctx->kfac, ctx->knots};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (auto &e : ctx->tev)
+        if (e) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -559,6 +562,7 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
         CKC(cudaEventCreate(&ctx->ev0));
         CKC(cudaEventCreate(&ctx->ev1));
+        for (auto &e : ctx->tev) CKC(cudaEventCreate(&e));
         CKC(cudaMalloc(&ctx->W, sizeof(double) * 2 * M * R));
         CKC(cudaMalloc(&ctx->conc, sizeof(double) * 4 * M * R));
         CKC(cudaMalloc(&ctx->DEV, sizeof(double) * 2 * M * R));
@@ -999,8 +1003,23 @@ scft_status scft_free_energy(scft_ctx *ctx, double *FE, double *FEs, double *FEs
     double fe = 0;
     scft_status s = free_energy(ctx, &fe);
     if (s != SCFT_OK) return s;
+    ctx->sf.FE = fe;
     const size_t n = sizeof(double) * ctx->strn;
     if (FE) *FE = fe;
+    if (FEs) std::memcpy(FEs, ctx->sf.FEs.data(), n);
+    if (FEs0) std::memcpy(FEs0, ctx->sf.FEs0.data(), n);
+    if (FEs1) std::memcpy(FEs1, ctx->sf.FEs1.data(), n);
+    if (phctot) std::memcpy(phctot, ctx->sf.phctot.data(), n);
+    if (alf) std::memcpy(alf, ctx->sf.alf.data(), n);
+    return SCFT_OK;
+}
+
+scft_status scft_last_free_energy(const scft_ctx *ctx, double *FE, double *FEs, double *FEs0,
+                                  double *FEs1, double *phctot, double *alf)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    const size_t n = sizeof(double) * ctx->strn;
+    if (FE) *FE = ctx->sf.FE;
     if (FEs) std::memcpy(FEs, ctx->sf.FEs.data(), n);
     if (FEs0) std::memcpy(FEs0, ctx->sf.FEs0.data(), n);
     if (FEs1) std::memcpy(FEs1, ctx->sf.FEs1.data(), n);
@@ -1073,6 +1092,23 @@ scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st)
 {
     if (!ctx || !st) return SCFT_BAD_INPUT;
     *st = ctx->stats;
+    return SCFT_OK;
+}
+
+scft_status scft_timer_mark(scft_ctx *ctx, int slot)
+{
+    if (!ctx || slot < 0 || slot > 3) return SCFT_BAD_INPUT;
+    CK(cudaEventRecord(ctx->tev[slot], ctx->st));
+    return SCFT_OK;
+}
+
+scft_status scft_timer_elapsed(scft_ctx *ctx, int a, int b, double *ms)
+{
+    if (!ctx || !ms || a < 0 || a > 3 || b < 0 || b > 3) return SCFT_BAD_INPUT;
+    CK(cudaEventSynchronize(ctx->tev[b]));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, ctx->tev[a], ctx->tev[b]));
+    *ms = f;
     return SCFT_OK;
 }
 

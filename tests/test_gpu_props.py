@@ -1,0 +1,108 @@
+"""CUDA propagator, density and spline kernels against the FP64 oracle through
+the C ABI (density::props, step::do_step, the spline services)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import scft_string_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [
+    ((8, 8, 8), (4.0, 4.0, 4.0), 20, 0.5, 1),
+    ((12, 10, 6), (3.0, 2.5, 2.0), 21, 0.45, 2),
+    ((6, 5, 9), (2.0, 2.0, 3.0), 17, 0.3, 1),
+    ((16, 12, 20), (4.0, 3.0, 5.0), 24, 0.4, 2),
+    ((14, 7, 10), (3.5, 1.75, 2.5), 12, 0.5, 2),
+]
+
+
+def fields(m, seed, amp=1.0):
+    rng = np.random.default_rng(seed)
+    return rng.normal(0, amp, m).ravel(), rng.normal(0, 0.5 * amp, m).ravel()
+
+
+@pytest.mark.parametrize("m,D,Ns,f,ens", GRIDS)
+def test_do_step_fp64(built_lib, m, D, Ns, f, ens):
+    M = int(np.prod(m))
+    wm, wp = fields(m, 1)
+    ctx = S.Context(m, D, Ns, chi=10, f=f, phidb=0.8, ens=ens, strn=1, dostring=0)
+    ctx.set_fields(0, wm, wp)
+    od = O.Density(m, D, Ns)
+    od.prepare(1.0 / Ns, np.concatenate([wm, wp]))
+    rng = np.random.default_rng(2)
+    qin = 1.0 + 0.3 * rng.normal(size=2 * M)
+    n1 = int(round(Ns * (round(Ns * f) / Ns)))
+    for s in [0, n1 - 1, n1, Ns - 1]:
+        ref = od.do_step(qin, s, n1, Ns - n1)
+        got = ctx.do_step(0, qin, s)
+        assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), s
+
+
+@pytest.mark.parametrize("m,D,Ns,f,ens", GRIDS)
+def test_props_fp64(built_lib, m, D, Ns, f, ens):
+    M = int(np.prod(m))
+    wm, wp = fields(m, 3, 2.0)
+    alpha, phic = 0.2, 0.8
+    od = O.Density(m, D, Ns)
+    w0 = np.zeros(6 * M)
+    w0[:M], w0[M:2 * M] = wm, wp
+    lnQ0, phis0 = od.props(w0, Ns, alpha, phic, f, ens)
+    dens = S.Density(m, D, Ns, ens, alpha, phic, f)
+    w1 = np.zeros(6 * M)
+    w1[:M], w1[M:2 * M] = wm, wp
+    lnQ1, phis1 = dens.props(w1, Ns, alpha, phic, f)
+    assert abs(lnQ1 - lnQ0) <= 1e-12 * max(1.0, abs(lnQ0))
+    assert np.allclose(phis1, phis0, rtol=1e-12, atol=1e-14)
+    assert np.abs(w1[2 * M:] - w0[2 * M:]).max() <= 1e-12 * np.abs(w0[2 * M:]).max()
+    # propagators
+    ctx = dens.ctx
+    n1 = int(round(Ns * (round(Ns * f) / Ns)))
+    for which, s in [(0, Ns), (1, Ns), (0, n1), (1, 3)]:
+        got = ctx.propagator(ctx.strn, which, s)
+        ref = od.q(which, s)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("m,D,Ns,f,ens", GRIDS[:3])
+def test_props_fp32_close_to_fp64(built_lib, m, D, Ns, f, ens):
+    M = int(np.prod(m))
+    wm, wp = fields(m, 5, 1.0)
+    alpha, phic = 0.2, 0.8
+    od = O.Density(m, D, Ns)
+    w0 = np.zeros(6 * M)
+    w0[:M], w0[M:2 * M] = wm, wp
+    lnQ0, phis0 = od.props(w0, Ns, alpha, phic, f, ens)
+    dens = S.Density(m, D, Ns, ens, alpha, phic, f, precision="fp32")
+    w1 = np.zeros(6 * M)
+    w1[:M], w1[M:2 * M] = wm, wp
+    lnQ1, phis1 = dens.props(w1, Ns, alpha, phic, f)
+    assert abs(lnQ1 - lnQ0) <= 2e-6 * max(1.0, abs(lnQ0))
+    assert np.abs(w1[2 * M:3 * M] - w0[2 * M:3 * M]).max() <= 1e-5
+
+
+def test_spline_services_fp64(built_lib):
+    rng = np.random.default_rng(7)
+    strn, m = 6, (4, 4, 4)
+    M = 64
+    ctx = S.Context(m, (2, 2, 2), 10, chi=10, f=0.5, phidb=0.8, ens=2, strn=strn)
+    x = np.array([0.0, 0.15, 0.3, 0.52, 0.8, 1.0])
+    xref = np.linspace(0, 1, strn)
+    Wm = rng.normal(size=(strn, M))
+    doiis = np.array([0, 1, 1, 1, 1, 0], np.int32)
+    ref = O.spline_derivs(x, Wm, doiis)
+    got = ctx.spline_derivs(x, Wm, doiis)
+    assert np.allclose(got[doiis == 1], ref[doiis == 1], rtol=1e-13, atol=1e-13)
+    ref = O.spline_redist(x, xref, Wm, doiis, 0.37)
+    got = ctx.spline_redist(x, xref, Wm, doiis, 0.37)
+    assert np.allclose(got, ref, rtol=1e-13, atol=1e-13)
+
+
+def test_bad_inputs_return_status(built_lib):
+    with pytest.raises(S.ScftError) as e:
+        S.Context((11, 8, 8), (2, 2, 2), 10, chi=10, f=0.5, phidb=0.8)
+    assert e.value.status == 3
+    ctx = S.Context((8, 8, 8), (2, 2, 2), 10, chi=10, f=0.5, phidb=0.8)
+    with pytest.raises(S.ScftError) as e:
+        ctx.props(5)
+    assert e.value.status == 3

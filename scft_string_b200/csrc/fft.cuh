@@ -326,3 +326,161 @@ __device__ void slab_inverse(cplx<T> *buf, const Geo &g, const cplx<T> *twy, con
 }
 
 }  // namespace scft
+
+// ===================================================================== fixed shapes
+// The same Stockham transforms with every length, line count, stride and
+// thread count known at compile time: index arithmetic folds to shifts and
+// multiplies and each thread's butterflies are fully unrolled.  Used for the
+// grid sizes the host has instantiations for; other sizes take the runtime
+// path above.
+namespace scft {
+
+__host__ __device__ constexpr int pick_radix(int rem)
+{
+    return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5 : 7;
+}
+
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, int R, int NS>
+__device__ __forceinline__ void fft_stage_fixed(cplx<T> *__restrict__ buf, const cplx<T> *__restrict__ tw,
+                                                int sign)
+{
+    constexpr int NR = N / R;
+    constexpr int NB = NLINES * NR;
+    constexpr int PER = (NB + NT - 1) / NT;
+    constexpr int TSTEP = N / (NS * R);
+    cplx<T> v[PER][R];
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+            const int k = j % NS;
+            const cplx<T> *src = buf + line * LS + j * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                cplx<T> a = src[r * NR * ES];
+                if (NS > 1 && r > 0) {
+                    const cplx<T> w = tw[r * k * TSTEP];
+                    a = sign < 0 ? cmul(a, w) : cmulc(a, w);
+                }
+                v[i][r] = a;
+            }
+            Dft<T, R>::run(v[i], sign, tw, N);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+            const int k = j % NS;
+            cplx<T> *dst = buf + line * LS + ((j - k) * R + k) * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[r * NS * ES] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, int NS = 1>
+__device__ __forceinline__ void fft_fixed(cplx<T> *buf, const cplx<T> *tw, int sign)
+{
+    if constexpr (NS < N) {
+        constexpr int R = pick_radix(N / NS);
+        fft_stage_fixed<T, N, NLINES, ES, LS, LF, NT, R, NS>(buf, tw, sign);
+        fft_fixed<T, N, NLINES, ES, LS, LF, NT, NS * R>(buf, tw, sign);
+    }
+}
+
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
+{
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, NW = NT / 32, TL = (MK2 + 31) / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+    for (int p = warp; p < NPAIR; p += NW) {
+        cplx<T> *row = buf + 2 * p * MK2;
+        const bool has_b = (2 * p + 1 < M1);
+        cplx<T> A[TL], B[TL];
+#pragma unroll
+        for (int t = 0; t < TL; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < MK2) {
+                const cplx<T> ck = row[kz];
+                const cplx<T> cm = row[kz == 0 ? 0 : M2 - kz];
+                A[t] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
+                B[t] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < TL; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < MK2) {
+                row[kz] = A[t];
+                if (has_b) row[MK2 + kz] = B[t];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
+{
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, NW = NT / 32, TL = (MK2 + 31) / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+    for (int p = warp; p < NPAIR; p += NW) {
+        cplx<T> *row = buf + 2 * p * MK2;
+        const bool has_b = (2 * p + 1 < M1);
+        cplx<T> A[TL], B[TL];
+#pragma unroll
+        for (int t = 0; t < TL; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < MK2) {
+                A[t] = row[kz];
+                B[t] = has_b ? row[MK2 + kz] : cplx<T>{(T)0, (T)0};
+                if (kz == 0 || 2 * kz == M2) {
+                    A[t].y = (T)0;
+                    B[t].y = (T)0;
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < TL; t++) {
+            const int kz = lane + 32 * t;
+            if (kz < MK2) {
+                row[kz] = {A[t].x - B[t].y, A[t].y + B[t].x};
+                if (kz > 0 && 2 * kz < M2) row[M2 - kz] = {A[t].x + B[t].y, B[t].x - A[t].y};
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
+{
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
+    fft_fixed<T, M2, NPAIR, 1, 2 * MK2, false, NT>(buf, twz, -1);
+    slab_unpack_fixed<T, M1, M2, NT>(buf);
+    __syncthreads();
+    fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, -1);
+}
+
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
+{
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
+    fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, +1);
+    slab_pack_fixed<T, M1, M2, NT>(buf);
+    __syncthreads();
+    fft_fixed<T, M2, NPAIR, 1, 2 * MK2, false, NT>(buf, twz, +1);
+}
+
+}  // namespace scft

@@ -47,7 +47,11 @@ struct PropsLaunch {
     int ew_blocks;   // elementwise grid (per slot)
     int red_blocks;  // reduction grid (per slot)
     int big;         // FFT kernels need more than 256 threads per CTA
+    int fixed;       // compile-time shape id (0: runtime-shaped kernels)
 };
+
+int fixed_shape_id(int m0, int m1, int m2);
+int fixed_shape_threads(int id);
 
 template <typename T>
 int launch_props(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st);

@@ -59,39 +59,71 @@ __global__ void k_prepare(PropsArgs<T> a)
     }
 }
 
+// ---------------------------------------------------------------- shape dispatch
+// FM0/FM1/FM2 = 0: sizes from the runtime Geo; otherwise compile-time sizes
+// (blockDim.x == MT, tile width from kTile<T>).
+template <typename T>
+struct kTile {
+    static constexpr int value = sizeof(T) == 4 ? 32 : 16;
+};
+
+template <typename T, int MT, int FM1, int FM2>
+__device__ __forceinline__ void slab_fwd(cplx<T> *buf, const Geo &g, const cplx<T> *twy,
+                                         const cplx<T> *twz, int *err)
+{
+    if constexpr (FM1 != 0)
+        slab_forward_fixed<T, FM1, FM2, MT>(buf, twy, twz);
+    else
+        slab_forward(buf, g, twy, twz, err);
+}
+
+template <typename T, int MT, int FM1, int FM2>
+__device__ __forceinline__ void slab_inv(cplx<T> *buf, const Geo &g, const cplx<T> *twy,
+                                         const cplx<T> *twz, int *err)
+{
+    if constexpr (FM1 != 0)
+        slab_inverse_fixed<T, FM1, FM2, MT>(buf, twy, twz);
+    else
+        slab_inverse(buf, g, twy, twz, err);
+}
+
 // ---------------------------------------------------------------- combine
 // mode 0: finishes step s (q(s+1) = Richardson combination);
 // mode 1: q(s+1) = 1 (Array_set_value, density.h:368-369; called with s = -1);
 // mode 2: q(s+1) is taken from the propagator store (single-step entry).
 // Then starts step s+1 when s+1 < Ns.
-template <typename T, int MT>
-__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> a, int s, int mode)
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) k_combine(PropsArgs<T> a, int s, int mode)
 {
     extern __shared__ unsigned char smem_raw[];
     const Geo &g = a.g;
+    constexpr bool FX = FM1 != 0;
+    const int m1 = FX ? FM1 : g.m1, m2 = FX ? FM2 : g.m2, mk2 = m2 / 2 + 1;
+    const int m0 = FX ? FM0 : g.m0, M = m0 * m1 * m2, Mk = m0 * m1 * mk2;
+    const int slab_c = m1 * mk2 + m2 + 32;
+    const int nthr = FX ? MT : (int)blockDim.x;
     cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *twy = buf + g.slab_c;
-    cplx<T> *twz = twy + g.m1;
-    load_tw(twy, a.tw + g.m0, g.m1);
-    load_tw(twz, a.tw + g.m0 + g.m1, g.m2);
+    cplx<T> *twy = buf + slab_c;
+    cplx<T> *twz = twy + m1;
+    for (int i = threadIdx.x; i < m1; i += nthr) twy[i] = a.tw[m0 + i];
+    for (int i = threadIdx.x; i < m2; i += nthr) twz[i] = a.tw[m0 + m1 + i];
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
-    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2, M = g.M;
     const size_t slab_r = (size_t)x * m1 * m2;  // real offset of this slab
     const size_t slab_k = (size_t)x * m1 * mk2;
     const T *etab = a.etab + (size_t)slot * 2 * M;
-    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
-    cplx<T> *specB = specA + g.Mk;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
+    cplx<T> *specB = specA + Mk;
     const int sn = s + 1;
     T *qn = a.hist + hist_off<T>(g, slot, sn, fld) + slab_r;
-    const int npz = g.npair * m2;
+    const int npair = (m1 + 1) / 2, npz = npair * m2;
 
     if (mode == 0) {
-        for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specA[slab_k + i];
+        for (int i = threadIdx.x; i < m1 * mk2; i += nthr) buf[i] = specA[slab_k + i];
         __syncthreads();
-        slab_inverse(buf, g, twy, twz, a.err);
+        slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
         const T *E4 = etab + (size_t)etab_sel(g, fld, s) * M + slab_r;
         const T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
-        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        for (int e = threadIdx.x; e < npz; e += nthr) {
             const int p = e / m2, z = e - p * m2;
             cplx<T> &c = buf[2 * p * mk2 + z];
             const int r0 = 2 * p * m2 + z;
@@ -107,7 +139,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> 
             }
         }
     } else if (mode == 1) {
-        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        for (int e = threadIdx.x; e < npz; e += nthr) {
             const int p = e / m2, z = e - p * m2;
             const int r0 = 2 * p * m2 + z;
             const bool hb = 2 * p + 1 < m1;
@@ -116,7 +148,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> 
             if (hb) qn[r0 + m2] = (T)1;
         }
     } else {
-        for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+        for (int e = threadIdx.x; e < npz; e += nthr) {
             const int p = e / m2, z = e - p * m2;
             const int r0 = 2 * p * m2 + z;
             const bool hb = 2 * p + 1 < m1;
@@ -127,7 +159,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> 
     __syncthreads();
     const T *E4n = etab + (size_t)etab_sel(g, fld, sn) * M + slab_r;
     // half step input E4' q'
-    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+    for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
         cplx<T> &c = buf[2 * p * mk2 + z];
         const int r0 = 2 * p * m2 + z;
@@ -135,11 +167,11 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> 
         if (2 * p + 1 < m1) c.y *= E4n[r0 + m2];
     }
     __syncthreads();
-    slab_forward(buf, g, twy, twz, a.err);
-    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specA[slab_k + i] = buf[i];
+    slab_fwd<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += nthr) specA[slab_k + i] = buf[i];
     __syncthreads();
     // full step input E2' q' (q' re-read from the propagator store written above)
-    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+    for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
         const int r0 = 2 * p * m2 + z;
         const T e0 = E4n[r0];
@@ -151,36 +183,40 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_combine(PropsArgs<T> 
         buf[2 * p * mk2 + z] = {v0, v1};
     }
     __syncthreads();
-    slab_forward(buf, g, twy, twz, a.err);
-    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specB[slab_k + i] = buf[i];
+    slab_fwd<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += nthr) specB[slab_k + i] = buf[i];
 }
 
 // ---------------------------------------------------------------- mid
-template <typename T, int MT>
-__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_mid(PropsArgs<T> a, int s)
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) k_mid(PropsArgs<T> a, int s)
 {
     extern __shared__ unsigned char smem_raw[];
     const Geo &g = a.g;
+    constexpr bool FX = FM1 != 0;
+    const int m1 = FX ? FM1 : g.m1, m2 = FX ? FM2 : g.m2, mk2 = m2 / 2 + 1;
+    const int m0 = FX ? FM0 : g.m0, M = m0 * m1 * m2, Mk = m0 * m1 * mk2;
+    const int slab_c = m1 * mk2 + m2 + 32;
+    const int nthr = FX ? MT : (int)blockDim.x;
     cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *twy = buf + g.slab_c;
-    cplx<T> *twz = twy + g.m1;
-    load_tw(twy, a.tw + g.m0, g.m1);
-    load_tw(twz, a.tw + g.m0 + g.m1, g.m2);
+    cplx<T> *twy = buf + slab_c;
+    cplx<T> *twz = twy + m1;
+    for (int i = threadIdx.x; i < m1; i += nthr) twy[i] = a.tw[m0 + i];
+    for (int i = threadIdx.x; i < m2; i += nthr) twz[i] = a.tw[m0 + m1 + i];
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
-    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2, M = g.M;
     const size_t slab_r = (size_t)x * m1 * m2;
     const size_t slab_k = (size_t)x * m1 * mk2;
     const T *E4 = a.etab + (size_t)slot * 2 * M + (size_t)etab_sel(g, fld, s) * M + slab_r;
-    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
-    cplx<T> *specB = specA + g.Mk;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
+    cplx<T> *specB = specA + Mk;
     T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
-    const int npz = g.npair * m2;
+    const int npz = ((m1 + 1) / 2) * m2;
 
     // full step: P = E2 * qs1
-    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specB[slab_k + i];
+    for (int i = threadIdx.x; i < m1 * mk2; i += nthr) buf[i] = specB[slab_k + i];
     __syncthreads();
-    slab_inverse(buf, g, twy, twz, a.err);
-    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+    slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
+    for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
         const cplx<T> c = buf[2 * p * mk2 + z];
         const int r0 = 2 * p * m2 + z;
@@ -193,10 +229,10 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_mid(PropsArgs<T> a, i
     }
     __syncthreads();
     // second half step input: E2 * (first half step)
-    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = specA[slab_k + i];
+    for (int i = threadIdx.x; i < m1 * mk2; i += nthr) buf[i] = specA[slab_k + i];
     __syncthreads();
-    slab_inverse(buf, g, twy, twz, a.err);
-    for (int e = threadIdx.x; e < npz; e += blockDim.x) {
+    slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
+    for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
         cplx<T> &c = buf[2 * p * mk2 + z];
         const int r0 = 2 * p * m2 + z;
@@ -210,48 +246,56 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_mid(PropsArgs<T> a, i
         }
     }
     __syncthreads();
-    slab_forward(buf, g, twy, twz, a.err);
-    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) specA[slab_k + i] = buf[i];
+    slab_fwd<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
+    for (int i = threadIdx.x; i < m1 * mk2; i += nthr) specA[slab_k + i] = buf[i];
 }
 
 // ---------------------------------------------------------------- pencil
 // x-transform of a tile of tc consecutive (ky, kz) columns, times the
 // diffusion factor (Mult_self, GPU_kernels.h:175-181), inverse x-transform.
 // both != 0: spectrum A with K2 and spectrum B with K1; else A with K2 only.
-template <typename T, int MT>
-__global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_pencil(PropsArgs<T> a, int both)
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) k_pencil(PropsArgs<T> a, int both)
 {
     extern __shared__ unsigned char smem_raw[];
     const Geo &g = a.g;
-    const int tc = g.tc, m0 = g.m0;
+    constexpr bool FX = FM0 != 0;
+    constexpr int TCF = kTile<T>::value;
+    const int tc = FX ? TCF : g.tc, m0 = FX ? FM0 : g.m0;
+    const int m1 = FX ? FM1 : g.m1, mk2 = (FX ? FM2 : g.m2) / 2 + 1;
+    const int Mk = m0 * m1 * mk2;
+    const int nthr = FX ? MT : (int)blockDim.x;
     cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
     cplx<T> *twx = buf + tc * m0;
     T *colf = reinterpret_cast<T *>(twx + m0);
     T *gx = colf + tc;
-    load_tw(twx, a.tw, m0);
+    for (int i = threadIdx.x; i < m0; i += nthr) twx[i] = a.tw[i];
     const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
-    const int ncol = g.m1 * g.mk2;
+    const int ncol = m1 * mk2;
     const int c0 = tile * tc;
-    for (int t = threadIdx.x; t < tc; t += blockDim.x) {
+    for (int t = threadIdx.x; t < tc; t += nthr) {
         const int c = c0 + t;
-        const int y = c / g.mk2, kz = c - y * g.mk2;
-        colf[t] = c < ncol ? a.kfac[m0 + y] * a.kfac[m0 + g.m1 + kz] : (T)0;
+        const int y = c / mk2, kz = c - y * mk2;
+        colf[t] = c < ncol ? a.kfac[m0 + y] * a.kfac[m0 + m1 + kz] : (T)0;
     }
-    for (int i = threadIdx.x; i < m0; i += blockDim.x) gx[i] = a.kfac[i];
+    for (int i = threadIdx.x; i < m0; i += nthr) gx[i] = a.kfac[i];
     const T invM = a.invM;
-    cplx<T> *spec = a.spec + ((size_t)slot * 2 + fld) * 2 * g.Mk;
+    cplx<T> *spec = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     const int npass = both ? 2 : 1;
     for (int pass = 0; pass < npass; pass++) {
-        cplx<T> *sp = spec + (size_t)pass * g.Mk;
+        cplx<T> *sp = spec + (size_t)pass * Mk;
         __syncthreads();
-        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        for (int e = threadIdx.x; e < tc * m0; e += nthr) {
             const int x = e / tc, t = e - x * tc;
             const int c = c0 + t;
             buf[e] = c < ncol ? sp[(size_t)x * ncol + c] : cplx<T>{(T)0, (T)0};
         }
         __syncthreads();
-        cta_fft(buf, g.px, tc, tc, 1, true, twx, -1, a.err);
-        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        if constexpr (FX)
+            fft_fixed<T, FM0, TCF, TCF, 1, true, MT>(buf, twx, -1);
+        else
+            cta_fft(buf, g.px, tc, tc, 1, true, twx, -1, a.err);
+        for (int e = threadIdx.x; e < tc * m0; e += nthr) {
             const int x = e / tc, t = e - x * tc;
             const T k2 = gx[x] * colf[t];
             // pass 0: K2 = g/M ; pass 1: K1 = g^2/M  (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
@@ -260,8 +304,11 @@ __global__ void __launch_bounds__(MT, MT == 256 ? 3 : 1) k_pencil(PropsArgs<T> a
             buf[e].y *= f;
         }
         __syncthreads();
-        cta_fft(buf, g.px, tc, tc, 1, true, twx, +1, a.err);
-        for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        if constexpr (FX)
+            fft_fixed<T, FM0, TCF, TCF, 1, true, MT>(buf, twx, +1);
+        else
+            cta_fft(buf, g.px, tc, tc, 1, true, twx, +1, a.err);
+        for (int e = threadIdx.x; e < tc * m0; e += nthr) {
             const int x = e / tc, t = e - x * tc;
             const int c = c0 + t;
             if (c < ncol) sp[(size_t)x * ncol + c] = buf[e];
@@ -427,20 +474,21 @@ __global__ void k_dfinal(PropsArgs<T> a, int nblk)
 }
 
 // ---------------------------------------------------------------- launchers
-// MT bounds the CTA size of the FFT kernels: 256 keeps the staged butterflies
-// in registers; 1024 serves slabs too large for 256 threads.
-template <typename T, int MT>
+// MT bounds the CTA size of the FFT kernels.  Shapes with compile-time
+// instantiations (cubic 32..128 and 64x64x96) use MT threads exactly; the
+// runtime-shaped kernels use 256 (or 1024 for slabs too large for 256).
+template <typename T, int MT, int F0, int F1, int F2>
 int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
 {
     const Geo &g = a.g;
     dim3 gs(g.m0, 2, nslots), gp(g.ncol_tiles, 2, nslots);
     k_prepare<T><<<dim3(L.ew_blocks, nslots), 256, 0, st>>>(a);
-    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, -1, 1);
+    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, -1, 1);
     for (int s = 0; s < g.Ns; s++) {
-        k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
-        k_mid<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
-        k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
-        k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+        k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
+        k_mid<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
+        k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
+        k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
     }
     k_qsum<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
     k_qfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
@@ -449,46 +497,80 @@ int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cud
     return 4 * g.Ns + 6;
 }
 
-template <typename T>
-int launch_props(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
-{
-    return L.big ? launch_props_mt<T, 1024>(a, L, nslots, st) : launch_props_mt<T, 256>(a, L, nslots, st);
-}
-
 // one contour step s of slot 0 starting from the propagator store slice s
-template <typename T, int MT>
+template <typename T, int MT, int F0, int F1, int F2>
 int launch_single_step_mt(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st)
 {
     const Geo &g = a.g;
     dim3 gs(g.m0, 2, 1), gp(g.ncol_tiles, 2, 1);
     k_prepare<T><<<dim3(L.ew_blocks, 1), 256, 0, st>>>(a);
-    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s - 1, 2);
-    k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
-    k_mid<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
-    k_pencil<T, MT><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
-    k_combine<T, MT><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s - 1, 2);
+    k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
+    k_mid<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
+    k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
+    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
     return 6;
+}
+
+template <typename T, int MT, int F0, int F1, int F2>
+int set_smem_mt(const PropsLaunch &L)
+{
+    cudaError_t e1 = cudaFuncSetAttribute(k_combine<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
+    cudaError_t e2 = cudaFuncSetAttribute(k_mid<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
+    cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : -1;
+}
+
+// op 0: props, 1: single step, 2: shared-memory attributes
+template <typename T, int MT, int F0, int F1, int F2>
+int run_op(int op, const PropsArgs<T> *a, const PropsLaunch &L, int n, cudaStream_t st)
+{
+    if (op == 0) return launch_props_mt<T, MT, F0, F1, F2>(*a, L, n, st);
+    if (op == 1) return launch_single_step_mt<T, MT, F0, F1, F2>(*a, L, n, st);
+    return set_smem_mt<T, MT, F0, F1, F2>(L);
+}
+
+template <typename T>
+int dispatch(int op, const PropsArgs<T> *a, const PropsLaunch &L, int n, cudaStream_t st)
+{
+    switch (L.fixed) {
+        case 32: return run_op<T, 256, 32, 32, 32>(op, a, L, n, st);
+        case 48: return run_op<T, 256, 48, 48, 48>(op, a, L, n, st);
+        case 64: return run_op<T, 256, 64, 64, 64>(op, a, L, n, st);
+        case 96: return run_op<T, 256, 96, 96, 96>(op, a, L, n, st);
+        case 128: return run_op<T, 512, 128, 128, 128>(op, a, L, n, st);
+        case 6496: return run_op<T, 256, 64, 64, 96>(op, a, L, n, st);
+        default: break;
+    }
+    return L.big ? run_op<T, 1024, 0, 0, 0>(op, a, L, n, st) : run_op<T, 256, 0, 0, 0>(op, a, L, n, st);
+}
+
+// compile-time shape id for a grid (0: runtime-shaped kernels)
+int fixed_shape_id(int m0, int m1, int m2)
+{
+    if (m0 == m1 && m1 == m2 && (m0 == 32 || m0 == 48 || m0 == 64 || m0 == 96 || m0 == 128)) return m0;
+    if (m0 == 64 && m1 == 64 && m2 == 96) return 6496;
+    return 0;
+}
+
+int fixed_shape_threads(int id) { return id == 128 ? 512 : 256; }
+
+template <typename T>
+int launch_props(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
+{
+    return dispatch<T>(0, &a, L, nslots, st);
 }
 
 template <typename T>
 int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st)
 {
-    return L.big ? launch_single_step_mt<T, 1024>(a, L, s, st) : launch_single_step_mt<T, 256>(a, L, s, st);
-}
-
-template <typename T, int MT>
-int set_smem_mt(const PropsLaunch &L)
-{
-    cudaError_t e1 = cudaFuncSetAttribute(k_combine<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
-    cudaError_t e2 = cudaFuncSetAttribute(k_mid<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
-    cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
-    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : -1;
+    return dispatch<T>(1, &a, L, s, st);
 }
 
 template <typename T>
 int set_props_smem(const PropsLaunch &L)
 {
-    return L.big ? set_smem_mt<T, 1024>(L) : set_smem_mt<T, 256>(L);
+    return dispatch<T>(2, nullptr, L, 0, nullptr);
 }
 
 template int launch_props<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -77,6 +78,10 @@ struct scft_ctx {
     void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
          *kfac = nullptr;
     SplineKnots *knots = nullptr;
+
+    // one captured CUDA graph per (chunk offset, batch size) of a props round
+    std::vector<cudaGraphExec_t> graphs;
+    bool use_graphs = true;
 
     // host state
     std::vector<int> doiis;
@@ -183,10 +188,28 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
     int launches = 0;
     for (size_t c0 = 0; c0 < reps.size(); c0 += ctx->nslots) {
         const int nb = (int)std::min<size_t>(ctx->nslots, reps.size() - c0);
-        if (ctx->prec == SCFT_FP32)
-            launches += launch_props<float>(props_args<float>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
-        else
-            launches += launch_props<double>(props_args<double>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+        auto launch = [&]() {
+            if (ctx->prec == SCFT_FP32)
+                return launch_props<float>(props_args<float>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+            return launch_props<double>(props_args<double>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+        };
+        const size_t key = (c0 <= (size_t)ctx->nrep_alloc) ? c0 * (ctx->nslots + 1) + nb : (size_t)-1;
+        if (ctx->use_graphs && key < ctx->graphs.size()) {
+            // the whole props round (4 Ns + 6 launches) replays as one graph
+            if (!ctx->graphs[key]) {
+                cudaGraph_t gr;
+                CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+                launch();
+                CK(cudaStreamEndCapture(ctx->st, &gr));
+                cudaError_t e = cudaGraphInstantiate(&ctx->graphs[key], gr, 0);
+                cudaGraphDestroy(gr);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+            }
+            CK(cudaGraphLaunch(ctx->graphs[key], ctx->st));
+            launches += 4 * ctx->g.Ns + 6;
+        } else {
+            launches += launch();
+        }
         for (int j = 0; j < nb; j++) {
             for (auto &so : ctx->slot_of)
                 if (so == j) so = -1;
@@ -466,6 +489,8 @@ void scft_destroy(scft_ctx *ctx)
         if (p) cudaFree(p);
     for (auto &e : ctx->tev)
         if (e) cudaEventDestroy(e);
+    for (auto &g : ctx->graphs)
+        if (g) cudaGraphExecDestroy(g);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -523,6 +548,8 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
                                                                       threads_for(g.py, g.mk2)))));
     L.pencil_threads = std::min(1024, std::max(128, round32(threads_for(g.px, g.tc))));
     L.big = (L.slab_threads > 256 || L.pencil_threads > 256) ? 1 : 0;
+    L.fixed = fixed_shape_id(g.m0, g.m1, g.m2);
+    if (L.fixed) L.slab_threads = L.pencil_threads = fixed_shape_threads(L.fixed);
     if (threads_for(g.pz, g.npair) > 1024 || threads_for(g.py, g.mk2) > 1024 ||
         threads_for(g.px, g.tc) > 1024) {
         delete ctx;
@@ -594,6 +621,8 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
             goto done;
         }
         ctx->doiis.assign(ctx->strn, 1);  // one process owns every replica (scft.cu:952-975)
+        ctx->graphs.assign((size_t)(R + 1) * (S + 1) + 1, nullptr);
+        if (const char *ev = getenv("SCFT_NO_GRAPHS")) ctx->use_graphs = ev[0] != '1';
         ctx->slot_of.assign(R, -1);
         ctx->rs_h.assign(kRsStride * R, 0.0);
         ctx->red_h.assign(ctx->nred_rows, 0.0);

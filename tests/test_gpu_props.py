@@ -106,3 +106,26 @@ def test_bad_inputs_return_status(built_lib):
     with pytest.raises(S.ScftError) as e:
         ctx.props(5)
     assert e.value.status == 3
+
+
+# grids with compile-time kernel instantiations
+FIXED = [(32, 32, 32), (48, 48, 48), (64, 64, 64), (96, 96, 96), (128, 128, 128), (64, 64, 96)]
+
+
+@pytest.mark.parametrize("m", FIXED)
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+def test_do_step_fixed_shapes(built_lib, m, prec, tol):
+    M = int(np.prod(m))
+    D = tuple(v / 16 for v in m)
+    Ns, f = 16, 0.5
+    wm, wp = fields(m, 11, 1.0)
+    ctx = S.Context(m, D, Ns, chi=10, f=f, phidb=0.8, ens=2, strn=1, dostring=0, precision=prec)
+    ctx.set_fields(0, wm, wp)
+    od = O.Density(m, D, Ns)
+    od.prepare(1.0 / Ns, np.concatenate([wm, wp]))
+    rng = np.random.default_rng(4)
+    qin = 1.0 + 0.3 * rng.normal(size=2 * M)
+    for s in [0, Ns - 1]:
+        ref = od.do_step(qin, s, 8, 8)
+        got = ctx.do_step(0, qin, s)
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (m, s)

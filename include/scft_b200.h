@@ -139,6 +139,18 @@ scft_status scft_free_energy(scft_ctx *ctx, double *FE, double *FEs, double *FEs
 scft_status scft_last_free_energy(const scft_ctx *ctx, double *FE, double *FEs, double *FEs0,
                                   double *FEs1, double *phctot, double *alf);
 
+/* ---- box, stress and parameter derivatives (no reference counterpart) -- */
+/* Box lengths D (the reference's D[3], used by setup_k_sq, density.h:79-95). */
+scft_status scft_set_box(scft_ctx *ctx, const double *D);
+scft_status scft_get_box(const scft_ctx *ctx, double *D);
+/* d lnQ/dL_i of replica ii at its current fields by the adjoint of the
+ * Richardson propagator (q^dagger is the adjoint of q's chain), and the box
+ * stress dF/dL_i = -d lnQ/dL_i, exact at a converged saddle point.  Either
+ * output may be NULL. */
+scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL);
+/* dF/d(chi N) of replica ii at a converged saddle point: 1/4 - <W-^2>/chi^2. */
+scft_status scft_dF_dchi(scft_ctx *ctx, int ii, double *out);
+
 /* ---- string spline services (host pointers) --------------------------- */
 /* density::splineDerivsChunked (density.h:491-508): ww[ii] -> W- of replica
  * ii; out[ii][r0..r0+n) = dW-/dalpha at knot x[ii] for doiis[ii] == 1. */

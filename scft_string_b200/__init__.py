@@ -73,7 +73,8 @@ EXPORTS = [
     "scft_do_step", "scft_get_propagator", "scft_solve_field0", "scft_solve_field0_all",
     "scft_solve_field", "scft_string_begin", "scft_string_step", "scft_string_end",
     "scft_free_energy", "scft_last_free_energy", "scft_spline_derivs", "scft_spline_redist", "scft_get_stats",
-    "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed",
+    "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
+    "scft_stress", "scft_dF_dchi",
 ]
 
 _lib = None
@@ -120,6 +121,10 @@ def lib():
     L.scft_get_stats.argtypes = [vp, C.POINTER(Stats)]
     L.scft_reset_stats.argtypes = [vp]
     L.scft_timer_mark.argtypes = [vp, C.c_int]
+    L.scft_set_box.argtypes = [vp, _dp]
+    L.scft_get_box.argtypes = [vp, _dp]
+    L.scft_stress.argtypes = [vp, C.c_int, _dp, _dp]
+    L.scft_dF_dchi.argtypes = [vp, C.c_int, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
     _lib = L
     return L
@@ -181,10 +186,15 @@ class Context:
         w = np.ascontiguousarray(np.concatenate([np.ravel(wm), np.ravel(wp)]), np.float64)
         self._ck(lib().scft_set_fields(self.h, int(ii), _p(w)))
 
-    def get_fields(self, ii):
-        w = np.zeros(2 * self.M)
+    def get_fields(self, ii, out=None):
+        """[W-, W+] of replica ii; `out` (2M float64, contiguous, may be pinned) is filled in place."""
+        w = np.zeros(2 * self.M) if out is None else out
         self._ck(lib().scft_get_fields(self.h, int(ii), _p(w)))
         return w
+
+    def set_fields_2m(self, ii, w2m):
+        """Replica ii's [W-, W+] from one contiguous 2M array (no staging copy)."""
+        self._ck(lib().scft_set_fields(self.h, int(ii), _p(w2m)))
 
     def get_conc(self, ii):
         c = np.zeros(4 * self.M)
@@ -301,6 +311,25 @@ class Context:
 
     def reset_stats(self):
         self._ck(lib().scft_reset_stats(self.h))
+
+    def set_box(self, D):
+        self._ck(lib().scft_set_box(self.h, _p(np.ascontiguousarray(D, np.float64))))
+
+    def get_box(self):
+        D = np.zeros(3)
+        self._ck(lib().scft_get_box(self.h, _p(D)))
+        return D
+
+    def stress(self, ii=0):
+        """(d lnQ/dL, dF/dL) of replica ii at its current fields (adjoint)."""
+        a, b = np.zeros(3), np.zeros(3)
+        self._ck(lib().scft_stress(self.h, int(ii), _p(a), _p(b)))
+        return a, b
+
+    def dF_dchi(self, ii=0):
+        v = C.c_double()
+        self._ck(lib().scft_dF_dchi(self.h, int(ii), C.byref(v)))
+        return v.value
 
     def timer_mark(self, slot):
         """Records CUDA event `slot` on the context's stream."""

@@ -12,8 +12,8 @@ LIB = os.path.join(HERE, "libscft_b200.so")
 EXE = os.path.join(HERE, "scft_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.h"]
+CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh"]
 
 
 def _stale(target, deps):
@@ -27,8 +27,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS]
     deps.append(os.path.join(ROOT, "include", "scft_b200.h"))
     if force or _stale(LIB, deps):
-        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-               "-o", LIB] + [os.path.join(CSRC, f) for f in CU_SOURCES]
+        # one nvcc per translation unit, in parallel, then one link
+        objdir = os.path.join(HERE, "_build")
+        os.makedirs(objdir, exist_ok=True)
+        objs, procs = [], []
+        for f in CU_SOURCES:
+            o = os.path.join(objdir, f.replace(".cu", ".o"))
+            objs.append(o)
+            cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-c",
+                   "-o", o, os.path.join(CSRC, f)]
+            if verbose:
+                print(" ".join(cmd))
+            procs.append(subprocess.Popen(cmd))
+        if any(p.wait() != 0 for p in procs):
+            raise RuntimeError("nvcc failed")
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB] + objs
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

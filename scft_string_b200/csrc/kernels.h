@@ -1,6 +1,7 @@
 // kernels.h -- launch interfaces between the host solver (scft_ctx.cu) and the
 // sm_100a kernels (props_kernels.cu, field_kernels.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -48,7 +49,14 @@ struct PropsLaunch {
     int red_blocks;  // reduction grid (per slot)
     int big;         // FFT kernels need more than 256 threads per CTA
     int fixed;       // compile-time shape id (0: runtime-shaped kernels)
+    int pf;          // prefetching (bulk-copy) slab kernels for the fixed shape
+    int mid_pf_smem, combine_pf_smem;
+    int tma_pencil;  // x pass through 2-D tensor-map tiles (fixed shapes)
+    int pencil_tma_smem;
+    const CUtensorMap *tmap;  // host copy of the spectrum tensor map
 };
+
+void pf_smem_bytes(int id, int fp32, int &mid, int &comb);
 
 int fixed_shape_id(int m0, int m1, int m2);
 int fixed_shape_threads(int id);
@@ -59,6 +67,36 @@ template <typename T>
 int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st);
 template <typename T>
 int set_props_smem(const PropsLaunch &L);
+
+// ------------------------------------------------------------------ stress (adjoint)
+constexpr int kStressPairs = 16;
+
+struct StressPairs {
+    int n;
+    int xs[kStressPairs], xf[kStressPairs];  // slice s and field (0 q, 1 q^dagger) of x
+    int ys[kStressPairs], yf[kStressPairs];  // of the adjoint y
+    int sel[kStressPairs];                   // E table of the step (0 A, 1 B)
+};
+
+template <typename T>
+struct StressArgs {
+    Geo g;
+    int slot;
+    const T *hist, *etab;
+    const cplx<T> *tw;
+    const T *kfac;
+    cplx<T> *S4, *S2, *S4p;  // [pair][x,y][Mk]
+    double *part;            // [pair][9][ntiles]
+    double L[3];
+    T invM;
+    int *err;
+};
+
+template <typename T>
+int launch_stress_chunk(const StressArgs<T> &a, const StressPairs &P, int slab_threads, int slab_smem,
+                        int pencil_threads, int pencil_smem, double *out, cudaStream_t st);
+template <typename T>
+int set_stress_smem(int slab_smem, int pencil_smem);
 
 // ------------------------------------------------------------------ FP64 field kernels
 constexpr int kMaxStrn = 64;

@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace scft {
 
@@ -316,6 +317,271 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     }
 }
 
+// ---------------------------------------------------------------- prefetching slab kernels
+// Compile-time shapes whose operands fit in shared memory.  One thread issues
+// bulk asynchronous copies (TMA, cp.async.bulk) of every slab the kernel needs
+// as soon as it starts; the transforms run while the later copies land, and
+// the epilogues read their operands from shared memory.
+// Shared-memory layout: [4 mbarriers | spectrum A | (spectrum B) | twiddles y, z |
+// real slabs].
+template <typename T, int M1, int M2>
+struct SlabSmem {
+    static constexpr int MK2 = M2 / 2 + 1;
+    static constexpr int SLAB_C = M1 * MK2 + M2 + 32;              // complex elements per spectrum buffer
+    static constexpr int SPEC_BYTES = M1 * MK2 * 2 * (int)sizeof(T); // bytes copied per spectrum slab
+    static constexpr int REAL = M1 * M2;                           // reals per real slab
+    static constexpr int REAL_BYTES = REAL * (int)sizeof(T);
+    static constexpr int BARS = 128;
+    static constexpr int mid_bytes() { return BARS + (2 * SLAB_C + M1 + M2) * 2 * (int)sizeof(T) + REAL_BYTES; }
+    static constexpr int combine_bytes() { return BARS + (SLAB_C + M1 + M2) * 2 * (int)sizeof(T) + 2 * REAL_BYTES; }
+};
+
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_mid_pf(PropsArgs<T> a, int s)
+{
+    using L = SlabSmem<T, FM1, FM2>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const Geo &g = a.g;
+    constexpr int m1 = FM1, m2 = FM2, mk2 = L::MK2, M = FM0 * FM1 * FM2, Mk = FM0 * FM1 * L::MK2;
+    constexpr int npz = ((m1 + 1) / 2) * m2;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw + L::BARS);
+    cplx<T> *bufB = bufA + L::SLAB_C;
+    cplx<T> *twy = bufB + L::SLAB_C;
+    cplx<T> *twz = twy + m1;
+    T *E4s = reinterpret_cast<T *>(twz + m2);
+    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
+    const T *E4g = a.etab + (size_t)slot * 2 * M + (size_t)etab_sel(g, fld, s) * M + slab_r;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
+    cplx<T> *specB = specA + Mk;
+    T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 3; i++) mbar_init(&bars[i], 1);
+        mbar_fence_init();
+        mbar_expect_tx(&bars[0], L::SPEC_BYTES);
+        bulk_g2s(bufB, specB + slab_k, L::SPEC_BYTES, &bars[0]);
+        mbar_expect_tx(&bars[1], L::REAL_BYTES);
+        bulk_g2s(E4s, E4g, L::REAL_BYTES, &bars[1]);
+        mbar_expect_tx(&bars[2], L::SPEC_BYTES);
+        bulk_g2s(bufA, specA + slab_k, L::SPEC_BYTES, &bars[2]);
+    }
+    for (int i = threadIdx.x; i < m1; i += MT) twy[i] = a.tw[FM0 + i];
+    for (int i = threadIdx.x; i < m2; i += MT) twz[i] = a.tw[FM0 + m1 + i];
+    __syncthreads();
+    // full step: P = E2 * qs1
+    mbar_wait(&bars[0], 0, a.err);
+    slab_inverse_fixed<T, m1, m2, MT>(bufB, twy, twz);
+    mbar_wait(&bars[1], 0, a.err);
+    for (int e = threadIdx.x; e < npz; e += MT) {
+        const int p = e / m2, z = e - p * m2;
+        const cplx<T> c = bufB[2 * p * mk2 + z];
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = E4s[r0];
+        P[r0] = c.x * (e0 * e0);
+        if (2 * p + 1 < m1) {
+            const T e1 = E4s[r0 + m2];
+            P[r0 + m2] = c.y * (e1 * e1);
+        }
+    }
+    // second half step input: E2 * (first half step)
+    mbar_wait(&bars[2], 0, a.err);
+    slab_inverse_fixed<T, m1, m2, MT>(bufA, twy, twz);
+    for (int e = threadIdx.x; e < npz; e += MT) {
+        const int p = e / m2, z = e - p * m2;
+        cplx<T> &c = bufA[2 * p * mk2 + z];
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = E4s[r0];
+        c.x *= e0 * e0;
+        if (2 * p + 1 < m1) {
+            const T e1 = E4s[r0 + m2];
+            c.y *= e1 * e1;
+        } else {
+            c.y = (T)0;
+        }
+    }
+    __syncthreads();
+    slab_forward_fixed<T, m1, m2, MT>(bufA, twy, twz);
+    for (int i = threadIdx.x; i < m1 * mk2; i += MT) specA[slab_k + i] = bufA[i];
+}
+
+// combine with prefetch: mode 0 (Richardson), 1 (q = 1), 2 (q from the store)
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_combine_pf(PropsArgs<T> a, int s, int mode)
+{
+    using L = SlabSmem<T, FM1, FM2>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const Geo &g = a.g;
+    constexpr int m1 = FM1, m2 = FM2, mk2 = L::MK2, M = FM0 * FM1 * FM2, Mk = FM0 * FM1 * L::MK2;
+    constexpr int npz = ((m1 + 1) / 2) * m2;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw + L::BARS);
+    cplx<T> *twy = buf + L::SLAB_C;
+    cplx<T> *twz = twy + m1;
+    T *Q = reinterpret_cast<T *>(twz + m2);  // P, then q'
+    T *E = Q + L::REAL;                        // E4 of step s (or of step s+1)
+    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
+    const T *etab = a.etab + (size_t)slot * 2 * M;
+    cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
+    cplx<T> *specB = specA + Mk;
+    const int sn = s + 1;
+    T *qn = a.hist + hist_off<T>(g, slot, sn, fld) + slab_r;
+    const bool next = sn < g.Ns;
+    const int sel_n = next ? etab_sel(g, fld, sn) : 0;
+    const int sel_s = mode == 0 ? etab_sel(g, fld, s) : sel_n;
+    // E holds the table of step s; the next step reads it from shared memory
+    // unless it switches blocks there (s+1 == n1 or n2), then from global
+    const bool e_next_shared = sel_s == sel_n;
+    const T *E4n_g = etab + (size_t)sel_n * M + slab_r;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 3; i++) mbar_init(&bars[i], 1);
+        mbar_fence_init();
+        if (mode == 0) {
+            mbar_expect_tx(&bars[0], L::SPEC_BYTES);
+            bulk_g2s(buf, specA + slab_k, L::SPEC_BYTES, &bars[0]);
+            mbar_expect_tx(&bars[1], L::REAL_BYTES);
+            bulk_g2s(Q, a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r, L::REAL_BYTES, &bars[1]);
+        } else if (mode == 2) {
+            mbar_expect_tx(&bars[1], L::REAL_BYTES);
+            bulk_g2s(Q, qn, L::REAL_BYTES, &bars[1]);
+        }
+        if (mode == 0 || next) {
+            mbar_expect_tx(&bars[2], L::REAL_BYTES);
+            bulk_g2s(E, etab + (size_t)sel_s * M + slab_r, L::REAL_BYTES, &bars[2]);
+        }
+    }
+    for (int i = threadIdx.x; i < m1; i += MT) twy[i] = a.tw[FM0 + i];
+    for (int i = threadIdx.x; i < m2; i += MT) twz[i] = a.tw[FM0 + m1 + i];
+    __syncthreads();
+    if (mode == 0) {
+        mbar_wait(&bars[0], 0, a.err);
+        slab_inverse_fixed<T, m1, m2, MT>(buf, twy, twz);
+        mbar_wait(&bars[1], 0, a.err);
+        mbar_wait(&bars[2], 0, a.err);
+        for (int e = threadIdx.x; e < npz; e += MT) {
+            const int p = e / m2, z = e - p * m2;
+            const cplx<T> c = buf[2 * p * mk2 + z];
+            const int r0 = 2 * p * m2 + z;
+            // Richardson, GPU_kernels.h:199-203
+            const T q0 = (c.x * E[r0] * (T)4 - Q[r0]) / (T)3;
+            Q[r0] = q0;
+            qn[r0] = q0;
+            if (2 * p + 1 < m1) {
+                const int r1 = r0 + m2;
+                const T q1 = (c.y * E[r1] * (T)4 - Q[r1]) / (T)3;
+                Q[r1] = q1;
+                qn[r1] = q1;
+            }
+        }
+    } else if (mode == 1) {
+        for (int r = threadIdx.x; r < m1 * m2; r += MT) {
+            Q[r] = (T)1;
+            qn[r] = (T)1;
+        }
+    } else {
+        mbar_wait(&bars[1], 0, a.err);
+    }
+    if (!next) return;
+    if (mode != 0) mbar_wait(&bars[2], 0, a.err);
+    __syncthreads();
+    const T *En = e_next_shared ? E : E4n_g;
+    // half step input E4' q'
+    for (int e = threadIdx.x; e < npz; e += MT) {
+        const int p = e / m2, z = e - p * m2;
+        const int r0 = 2 * p * m2 + z;
+        const bool hb = 2 * p + 1 < m1;
+        buf[2 * p * mk2 + z] = {Q[r0] * En[r0], hb ? Q[r0 + m2] * En[r0 + m2] : (T)0};
+    }
+    __syncthreads();
+    slab_forward_fixed<T, m1, m2, MT>(buf, twy, twz);
+    for (int i = threadIdx.x; i < m1 * mk2; i += MT) specA[slab_k + i] = buf[i];
+    __syncthreads();
+    // full step input E2' q'
+    for (int e = threadIdx.x; e < npz; e += MT) {
+        const int p = e / m2, z = e - p * m2;
+        const int r0 = 2 * p * m2 + z;
+        const T e0 = En[r0];
+        T v1 = (T)0;
+        if (2 * p + 1 < m1) {
+            const T e1 = En[r0 + m2];
+            v1 = Q[r0 + m2] * (e1 * e1);
+        }
+        buf[2 * p * mk2 + z] = {Q[r0] * (e0 * e0), v1};
+    }
+    __syncthreads();
+    slab_forward_fixed<T, m1, m2, MT>(buf, twy, twz);
+    for (int i = threadIdx.x; i < m1 * mk2; i += MT) specB[slab_k + i] = buf[i];
+}
+
+// ---------------------------------------------------------------- TMA pencil
+// The x pass of a compile-time shape with the column tiles moved by 2-D
+// tensor-map copies: the spectra of every slot are one 2-D array of
+// (nslots*2*2*m0) rows by 2*m1*mk2 reals; a tile is the box {2*tc, m0}.
+// Both spectra of a both-pass are requested at kernel start, so the second
+// one lands while the first is transformed; results leave through tile stores.
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
+    k_pencil_tma(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int both)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr int TC = kTile<T>::value, m0 = FM0, m1 = FM1, mk2 = FM2 / 2 + 1;
+    constexpr int BOX = TC * m0;                      // complex elements per tile
+    constexpr uint32_t BOX_BYTES = BOX * 2 * sizeof(T);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw + 128);
+    cplx<T> *bufB = bufA + BOX;
+    cplx<T> *twx = bufB + BOX;
+    T *colf = reinterpret_cast<T *>(twx + m0);
+    T *gx = colf + TC;
+    const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
+    const int ncol = m1 * mk2, c0 = tile * TC;
+    const int x = 2 * c0;
+    const int y0 = ((slot * 2 + fld) * 2) * m0;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+        mbar_expect_tx(&bars[0], BOX_BYTES);
+        tma_load_2d(bufA, &tmap, x, y0, &bars[0]);
+        if (both) {
+            mbar_expect_tx(&bars[1], BOX_BYTES);
+            tma_load_2d(bufB, &tmap, x, y0 + m0, &bars[1]);
+        }
+    }
+    for (int i = threadIdx.x; i < m0; i += MT) {
+        twx[i] = a.tw[i];
+        gx[i] = a.kfac[i];
+    }
+    for (int t = threadIdx.x; t < TC; t += MT) {
+        const int c = c0 + t;
+        const int yy = c / mk2, kz = c - yy * mk2;
+        colf[t] = c < ncol ? a.kfac[m0 + yy] * a.kfac[m0 + m1 + kz] : (T)0;
+    }
+    __syncthreads();
+    const T invM = a.invM;
+    const int npass = both ? 2 : 1;
+    for (int pass = 0; pass < npass; pass++) {
+        cplx<T> *buf = pass == 0 ? bufA : bufB;
+        mbar_wait(&bars[pass], 0, a.err);
+        fft_fixed<T, m0, TC, TC, 1, true, MT>(buf, twx, -1);
+        for (int e = threadIdx.x; e < BOX; e += MT) {
+            const int xx = e / TC, t = e - xx * TC;
+            const T k2 = gx[xx] * colf[t];
+            // pass 0: K2 = g/M ; pass 1: K1 = g^2/M  (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
+            const T f = pass == 0 ? k2 * invM : (k2 * invM) * (k2 * invM) * a.Mreal;
+            buf[e].x *= f;
+            buf[e].y *= f;
+        }
+        __syncthreads();
+        fft_fixed<T, m0, TC, TC, 1, true, MT>(buf, twx, +1);
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) tma_store_2d(&tmap, x, y0 + pass * m0, buf);
+    }
+    if (threadIdx.x == 0) tma_store_wait_read();
+}
+
 // ---------------------------------------------------------------- Q and densities
 __device__ __forceinline__ double block_sum(double v, double *sh)
 {
@@ -478,17 +744,53 @@ __global__ void k_dfinal(PropsArgs<T> a, int nblk)
 // instantiations (cubic 32..128 and 64x64x96) use MT threads exactly; the
 // runtime-shaped kernels use 256 (or 1024 for slabs too large for 256).
 template <typename T, int MT, int F0, int F1, int F2>
+void launch_combine(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s, int mode, cudaStream_t st)
+{
+    if constexpr (F1 != 0) {
+        if (L.pf) {
+            k_combine_pf<T, MT, F0, F1, F2><<<gs, MT, L.combine_pf_smem, st>>>(a, s, mode);
+            return;
+        }
+    }
+    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, mode);
+}
+
+template <typename T, int MT, int F0, int F1, int F2>
+void launch_mid(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s, cudaStream_t st)
+{
+    if constexpr (F1 != 0) {
+        if (L.pf) {
+            k_mid_pf<T, MT, F0, F1, F2><<<gs, MT, L.mid_pf_smem, st>>>(a, s);
+            return;
+        }
+    }
+    k_mid<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
+}
+
+template <typename T, int MT, int F0, int F1, int F2>
+void launch_pencil(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gp, int both, cudaStream_t st)
+{
+    if constexpr (F1 != 0) {
+        if (L.tma_pencil) {
+            k_pencil_tma<T, MT, F0, F1, F2><<<gp, MT, L.pencil_tma_smem, st>>>(*L.tmap, a, both);
+            return;
+        }
+    }
+    k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, both);
+}
+
+template <typename T, int MT, int F0, int F1, int F2>
 int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cudaStream_t st)
 {
     const Geo &g = a.g;
     dim3 gs(g.m0, 2, nslots), gp(g.ncol_tiles, 2, nslots);
     k_prepare<T><<<dim3(L.ew_blocks, nslots), 256, 0, st>>>(a);
-    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, -1, 1);
+    launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
     for (int s = 0; s < g.Ns; s++) {
-        k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
-        k_mid<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
-        k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
-        k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 1, st);
+        launch_mid<T, MT, F0, F1, F2>(a, L, gs, s, st);
+        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 0, st);
+        launch_combine<T, MT, F0, F1, F2>(a, L, gs, s, 0, st);
     }
     k_qsum<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
     k_qfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
@@ -504,11 +806,11 @@ int launch_single_step_mt(const PropsArgs<T> &a, const PropsLaunch &L, int s, cu
     const Geo &g = a.g;
     dim3 gs(g.m0, 2, 1), gp(g.ncol_tiles, 2, 1);
     k_prepare<T><<<dim3(L.ew_blocks, 1), 256, 0, st>>>(a);
-    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s - 1, 2);
-    k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 1);
-    k_mid<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s);
-    k_pencil<T, MT, F0, F1, F2><<<gp, L.pencil_threads, L.pencil_smem, st>>>(a, 0);
-    k_combine<T, MT, F0, F1, F2><<<gs, L.slab_threads, L.slab_smem, st>>>(a, s, 0);
+    launch_combine<T, MT, F0, F1, F2>(a, L, gs, s - 1, 2, st);
+    launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 1, st);
+    launch_mid<T, MT, F0, F1, F2>(a, L, gs, s, st);
+    launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 0, st);
+    launch_combine<T, MT, F0, F1, F2>(a, L, gs, s, 0, st);
     return 6;
 }
 
@@ -518,7 +820,39 @@ int set_smem_mt(const PropsLaunch &L)
     cudaError_t e1 = cudaFuncSetAttribute(k_combine<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
     cudaError_t e2 = cudaFuncSetAttribute(k_mid<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
     cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
-    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : -1;
+    cudaError_t e4 = cudaSuccess, e5 = cudaSuccess;
+    if constexpr (F1 != 0) {
+        if (L.tma_pencil)
+            e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem);
+        if (e4 == cudaSuccess && L.pf) {
+            e4 = cudaFuncSetAttribute(k_combine_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.combine_pf_smem);
+            e5 = cudaFuncSetAttribute(k_mid_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.mid_pf_smem);
+        }
+    }
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess && e5 == cudaSuccess) ? 0 : -1;
+}
+
+// shared-memory bytes of the prefetching slab kernels for a fixed shape
+template <typename T>
+void pf_smem(int id, int &mid, int &comb)
+{
+    switch (id) {
+        case 32: mid = SlabSmem<T, 32, 32>::mid_bytes(); comb = SlabSmem<T, 32, 32>::combine_bytes(); return;
+        case 48: mid = SlabSmem<T, 48, 48>::mid_bytes(); comb = SlabSmem<T, 48, 48>::combine_bytes(); return;
+        case 64: mid = SlabSmem<T, 64, 64>::mid_bytes(); comb = SlabSmem<T, 64, 64>::combine_bytes(); return;
+        case 96: mid = SlabSmem<T, 96, 96>::mid_bytes(); comb = SlabSmem<T, 96, 96>::combine_bytes(); return;
+        case 128: mid = SlabSmem<T, 128, 128>::mid_bytes(); comb = SlabSmem<T, 128, 128>::combine_bytes(); return;
+        case 6496: mid = SlabSmem<T, 64, 96>::mid_bytes(); comb = SlabSmem<T, 64, 96>::combine_bytes(); return;
+        default: mid = comb = 0;
+    }
+}
+
+void pf_smem_bytes(int id, int fp32, int &mid, int &comb)
+{
+    if (fp32)
+        pf_smem<float>(id, mid, comb);
+    else
+        pf_smem<double>(id, mid, comb);
 }
 
 // op 0: props, 1: single step, 2: shared-memory attributes

@@ -6,6 +6,7 @@
 // mixing) runs on the device; the host keeps only the per-replica scalars
 // the reference keeps (errors, mixing parameters, arc-length knots) and
 // evaluates them in FP64 in the reference's order.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,6 +79,11 @@ struct scft_ctx {
     void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
          *kfac = nullptr;
     SplineKnots *knots = nullptr;
+    CUtensorMap tmap;  // spectra as a 2-D array for the x-pencil tiles
+    // adjoint (stress) scratch, allocated on first use
+    void *st_S4 = nullptr, *st_S2 = nullptr, *st_S4p = nullptr;
+    double *st_part = nullptr, *st_out = nullptr;
+    int rt_slab_threads = 0, rt_slab_smem = 0, rt_pencil_threads = 0, rt_pencil_smem = 0;
 
     // one captured CUDA graph per (chunk offset, batch size) of a props round
     std::vector<cudaGraphExec_t> graphs;
@@ -484,7 +490,8 @@ void scft_destroy(scft_ctx *ctx)
     if (!ctx) return;
     void *ptrs[] = {ctx->W, ctx->conc, ctx->DEV, ctx->dWda, ctx->rs, ctx->partials, ctx->redout,
                     ctx->rep_dev, ctx->err, ctx->etab, ctx->hist, ctx->spec, ctx->pbuf, ctx->tw,
-                    ctx->kfac, ctx->knots};
+                    ctx->kfac, ctx->knots, ctx->st_S4, ctx->st_S2, ctx->st_S4p, ctx->st_part,
+                    ctx->st_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : ctx->tev)
@@ -548,8 +555,15 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
                                                                       threads_for(g.py, g.mk2)))));
     L.pencil_threads = std::min(1024, std::max(128, round32(threads_for(g.px, g.tc))));
     L.big = (L.slab_threads > 256 || L.pencil_threads > 256) ? 1 : 0;
+    const int rt_slab_threads = L.slab_threads, rt_pencil_threads = L.pencil_threads;
     L.fixed = fixed_shape_id(g.m0, g.m1, g.m2);
     if (L.fixed) L.slab_threads = L.pencil_threads = fixed_shape_threads(L.fixed);
+    L.pf = 0;
+    if (L.fixed) {
+        pf_smem_bytes(L.fixed, T == 4, L.mid_pf_smem, L.combine_pf_smem);
+        L.pf = (std::max(L.mid_pf_smem, L.combine_pf_smem) <= (int)prop.sharedMemPerBlockOptin) ? 1 : 0;
+        if (const char *ev = getenv("SCFT_NO_PREFETCH")) L.pf = ev[0] == '1' ? 0 : L.pf;
+    }
     if (threads_for(g.pz, g.npair) > 1024 || threads_for(g.py, g.mk2) > 1024 ||
         threads_for(g.px, g.tc) > 1024) {
         delete ctx;
@@ -564,6 +578,10 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         return SCFT_BAD_INPUT;
     }
     ctx->g = g;
+    ctx->rt_slab_threads = rt_slab_threads;
+    ctx->rt_pencil_threads = rt_pencil_threads;
+    ctx->rt_slab_smem = L.slab_smem;
+    ctx->rt_pencil_smem = (int)((2 * g.tc * g.m0 + g.m0) * 2 * T);
     scft_status rc = SCFT_OK;
     auto fail = [&](cudaError_t e, const char *what) {
         ctx->lasterr = std::string(what) + ": " + cudaGetErrorString(e);
@@ -615,6 +633,33 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMemset(ctx->dWda, 0, sizeof(double) * M * R));
         CKC(cudaMemset(ctx->rs, 0, sizeof(double) * kRsStride * R));
         CKC(cudaMemset(ctx->err, 0, sizeof(int)));
+        // 2-D tensor map of all spectra: rows of 2*m1*mk2 reals, nslots*2*2*m0 rows
+        L.tma_pencil = 0;
+        if (L.fixed && !getenv("SCFT_NO_TMA_PENCIL")) {
+            typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                         const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                         CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                         CUtensorMapFloatOOBfill);
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess && fn) {
+                const int tc = T == 4 ? 32 : 16;
+                cuuint64_t dims[2] = {(cuuint64_t)2 * g.m1 * g.mk2, (cuuint64_t)S * 2 * 2 * g.m0};
+                cuuint64_t strides[1] = {(cuuint64_t)2 * g.m1 * g.mk2 * T};
+                cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)g.m0};
+                cuuint32_t es[2] = {1, 1};
+                CUresult r = ((EncodeFn)fn)(&ctx->tmap, T == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                                            2, ctx->spec, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r == CUDA_SUCCESS && g.m0 <= 256 && (strides[0] % 16) == 0) {
+                    L.tma_pencil = 1;
+                    L.tmap = &ctx->tmap;
+                    L.pencil_tma_smem = (int)(128 + (2 * tc * g.m0 + g.m0) * 2 * T + (tc + g.m0) * T);
+                }
+            }
+        }
         if ((T == 4 ? set_props_smem<float>(L) : set_props_smem<double>(L)) != 0) {
             ctx->lasterr = "cudaFuncSetAttribute(max dynamic shared memory) failed";
             rc = SCFT_CUDA_ERROR;
@@ -1115,6 +1160,130 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
 {
     if (!ww || !xref || !doiis) return SCFT_BAD_INPUT;
     return spline_host(ctx, x, xref, nullptr, nullptr, ww, r0, n, doiis, lambda);
+}
+
+// box lengths: re-derive the per-axis diffusion factors (setup_k_sq, density.h:79-95)
+scft_status scft_set_box(scft_ctx *ctx, const double *D)
+{
+    if (!ctx || !D || !(D[0] > 0) || !(D[1] > 0) || !(D[2] > 0)) return SCFT_BAD_INPUT;
+    for (int i = 0; i < 3; i++) ctx->p.D[i] = D[i];
+    std::vector<unsigned char> twb, kfb;
+    if (ctx->prec == SCFT_FP32)
+        upload_tables<float>(ctx, twb, kfb);
+    else
+        upload_tables<double>(ctx, twb, kfb);
+    CK(cudaMemcpyAsync(ctx->kfac, kfb.data(), kfb.size(), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
+scft_status scft_get_box(const scft_ctx *ctx, double *D)
+{
+    if (!ctx || !D) return SCFT_BAD_INPUT;
+    for (int i = 0; i < 3; i++) D[i] = ctx->p.D[i];
+    return SCFT_OK;
+}
+
+// d lnQ / d L_i of replica ii at its current fields, by the adjoint of the
+// propagator (stress_kernels.cu); the free energy's box derivative at the
+// saddle point is dF/dL = -dlnQ/dL (the field terms carry no explicit L).
+scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    if (!ctx->st_S4) {
+        const size_t sz = T * 2 * 2 * (size_t)g.Mk * kStressPairs;
+        CK(cudaMalloc(&ctx->st_S4, sz));
+        CK(cudaMalloc(&ctx->st_S2, sz));
+        CK(cudaMalloc(&ctx->st_S4p, sz));
+        CK(cudaMalloc(&ctx->st_part, sizeof(double) * 9 * (size_t)g.ncol_tiles * kStressPairs));
+        CK(cudaMalloc(&ctx->st_out, sizeof(double) * 3 * kStressPairs));
+        if ((T == 4 ? set_stress_smem<float>(ctx->rt_slab_smem, ctx->rt_pencil_smem)
+                    : set_stress_smem<double>(ctx->rt_slab_smem, ctx->rt_pencil_smem)) != 0) {
+            ctx->lasterr = "stress kernels: shared memory attribute";
+            return SCFT_CUDA_ERROR;
+        }
+    }
+    // fresh propagators of replica ii
+    scft_status s = props_list(ctx, {ii});
+    if (s != SCFT_OK) return s;
+    const int slot = ctx->slot_of[ii];
+    const double Q2 = rsv(ctx, ii, kRsQ2), QC = rsv(ctx, ii, kRsQC);
+    // pairs: copolymer (q(s), q^dagger(N-1-s)), homopolymer (q^dagger(j), q^dagger(Nh-1-j))
+    struct Pr { int xs, xf, ys, yf, sel, homo; };
+    std::vector<Pr> pairs;
+    for (int s2 = 0; s2 < g.Ns; s2++) pairs.push_back({s2, 0, g.Ns - 1 - s2, 1, s2 < g.n1 ? 0 : 1, 0});
+    for (int j = 0; j < g.Nh; j++) pairs.push_back({j, 1, g.Nh - 1 - j, 1, 1, 1});
+    double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
+    std::vector<double> out(3 * kStressPairs);
+    for (size_t c0 = 0; c0 < pairs.size(); c0 += kStressPairs) {
+        StressPairs P;
+        std::memset(&P, 0, sizeof(P));
+        P.n = (int)std::min<size_t>(kStressPairs, pairs.size() - c0);
+        for (int p = 0; p < P.n; p++) {
+            const Pr &q = pairs[c0 + p];
+            P.xs[p] = q.xs;
+            P.xf[p] = q.xf;
+            P.ys[p] = q.ys;
+            P.yf[p] = q.yf;
+            P.sel[p] = q.sel;
+        }
+        int nl;
+        if (T == 4) {
+            StressArgs<float> a{g, slot, (const float *)ctx->hist, (const float *)ctx->etab,
+                                (const cplx<float> *)ctx->tw, (const float *)ctx->kfac,
+                                (cplx<float> *)ctx->st_S4, (cplx<float> *)ctx->st_S2,
+                                (cplx<float> *)ctx->st_S4p, ctx->st_part,
+                                {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, (float)(1.0 / g.M), ctx->err};
+            nl = launch_stress_chunk<float>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
+                                            ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
+        } else {
+            StressArgs<double> a{g, slot, (const double *)ctx->hist, (const double *)ctx->etab,
+                                 (const cplx<double> *)ctx->tw, (const double *)ctx->kfac,
+                                 (cplx<double> *)ctx->st_S4, (cplx<double> *)ctx->st_S2,
+                                 (cplx<double> *)ctx->st_S4p, ctx->st_part,
+                                 {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, 1.0 / g.M, ctx->err};
+            nl = launch_stress_chunk<double>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
+                                             ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
+        }
+        ctx->stats.kernel_launches += nl;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out.data(), ctx->st_out, sizeof(double) * 3 * P.n, cudaMemcpyDeviceToHost, ctx->st));
+        s = check_device_err(ctx);
+        if (s != SCFT_OK) return s;
+        for (int p = 0; p < P.n; p++)
+            for (int i = 0; i < 3; i++) (pairs[c0 + p].homo ? dQ2 : dQC)[i] += out[3 * p + i];
+    }
+    const double invM = 1.0 / g.M, phic = ctx->p.phidb, alpha = ctx->p.alpha;
+    for (int i = 0; i < 3; i++) {
+        dQC[i] *= invM;
+        dQ2[i] *= invM;
+        double d;
+        if (ctx->p.ens == 1)  // lnQ = phic ln QC + (1-phic)/alpha ln Q2 (density.h:390)
+            d = phic * dQC[i] / QC + ((1.0 - phic) / alpha) * dQ2[i] / Q2;
+        else                  // "lnQ" = Q2 + phic QC (density.h:398)
+            d = dQ2[i] + phic * dQC[i];
+        if (dlnQ_dL) dlnQ_dL[i] = d;
+        if (dF_dL) dF_dL[i] = -d;
+    }
+    return SCFT_OK;
+}
+
+// dF/d(chi N) at the saddle point: F = -lnQ + <W-^2>/chi - <W+> + chi/4 there
+// (the reference's F, scft.cu:823-826, with chi (phiB - phiA) = 2 W- and
+// phiA + phiB = 1), so dF/dchi = 1/4 - <W-^2>/chi^2.
+scft_status scft_dF_dchi(scft_ctx *ctx, int ii, double *out)
+{
+    if (!ctx || !out || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    std::vector<double> w(2 * (size_t)ctx->M);
+    scft_status s = scft_get_fields(ctx, ii, w.data());
+    if (s != SCFT_OK) return s;
+    double q = 0;
+    for (int r = 0; r < ctx->M; r++) q += w[r] * w[r];
+    q /= ctx->M;
+    *out = 0.25 - q / (ctx->p.chi * ctx->p.chi);
+    return SCFT_OK;
 }
 
 scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st)

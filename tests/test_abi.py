@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def header_functions():
     txt = open(os.path.join(ROOT, "include", "scft_b200.h")).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(scft_[a-z0-9_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(scft_[A-Za-z0-9_]+)\s*\(", txt)))
 
 
 def test_library_exports_every_header_symbol(built_lib):

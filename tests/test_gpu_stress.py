@@ -1,0 +1,91 @@
+"""Box stress and parameter derivatives (no reference code): the adjoint
+d lnQ/dL against central finite differences of the reference discretisation
+(h = 1e-4, FP64), the FP32 adjoint against the FP64 adjoint, and dF/dL,
+dF/dchiN at a converged saddle point against finite differences of
+re-converged free energies."""
+import numpy as np
+import pytest
+
+import scft_string_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+
+def smooth_fields(m, D, seed, amp=3.0):
+    rng = np.random.default_rng(seed)
+    x = [np.arange(m[i]) * D[i] / m[i] for i in range(3)]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    wm = amp * (np.cos(2 * np.pi * X / D[0]) + 0.5 * np.sin(2 * np.pi * Y / D[1]) * np.cos(2 * np.pi * Z / D[2]))
+    wm += 0.2 * rng.normal(size=m)
+    wp = 0.3 * rng.normal(size=m)
+    return wm.ravel(), wp.ravel()
+
+
+def lnq_at(ctx, D):
+    ctx.set_box(D)
+    ctx.props(0)
+    return ctx.get_conc(0)[1]
+
+
+@pytest.mark.parametrize("m,D,N,ens", [((8, 12, 10), (2.0, 3.0, 2.5), 20, 1),
+                                        ((12, 8, 16), (3.1, 2.2, 4.0), 24, 2),
+                                        ((32, 32, 32), (4.0, 4.0, 4.0), 40, 1)])
+def test_adjoint_matches_finite_differences(built_lib, m, D, N, ens):
+    D = np.array(D)
+    wm, wp = smooth_fields(m, D, 1)
+    ctx = S.Context(m, D, N, chi=12, f=0.45, phidb=0.8, ens=ens, alpha=0.1, strn=1, dostring=0)
+    ctx.set_fields(0, wm, wp)
+    dlnq, dF = ctx.stress(0)
+    assert np.allclose(dF, -dlnq)
+    h = 1e-4
+    for i in range(3):
+        Dp, Dm = D.copy(), D.copy()
+        Dp[i] += h
+        Dm[i] -= h
+        fd = (lnq_at(ctx, Dp) - lnq_at(ctx, Dm)) / (2 * h)
+        assert abs(dlnq[i] - fd) <= 1e-6 * max(1.0, abs(fd)), (i, dlnq[i], fd)
+    ctx.set_box(D)
+    # FP32 adjoint against the FP64 one
+    c32 = S.Context(m, D, N, chi=12, f=0.45, phidb=0.8, ens=ens, alpha=0.1, strn=1, dostring=0,
+                    precision="fp32")
+    c32.set_fields(0, wm, wp)
+    d32, _ = c32.stress(0)
+    assert np.allclose(d32, dlnq, rtol=2e-4, atol=2e-6)
+
+
+def converged(m, D, N, chi, iters=400):
+    ctx = S.Context(m, D, N, chi=chi, f=0.5, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0)
+    wm, wp = smooth_fields(m, D, 2, amp=0.3 * chi)
+    ctx.set_fields(0, wm, wp)
+    ctx.solve_field0_all(5000, 1e-10)
+    k, recs, _, _ = ctx.solve_field(iters, errTol=1e-3)
+    ctx.solve_field0(0, 5000, 1e-12)
+    ctx.props(0)
+    conc, lnQ, _ = ctx.get_conc(0)
+    W = ctx.get_fields(0)
+    M = ctx.M
+    pA, pB = conc[:M], conc[M:2 * M]
+    wa, wb = W[:M] + W[M:], W[M:] - W[:M]
+    F = -lnQ + np.mean(chi * pA * pB - wa * pA - wb * pB)
+    return ctx, F, recs[-1]["errtot"]
+
+
+def test_saddle_point_stress_and_dchi(built_lib):
+    m, N, chi = (16, 16, 16), 20, 12.0
+    D = np.array([3.6, 3.6, 3.6])
+    ctx, F0, err = converged(m, D, N, chi)
+    assert err < 1e-7
+    _, dF = ctx.stress(0)
+    h = 1e-3
+    Dp, Dm = D.copy(), D.copy()
+    Dp[0] += h
+    Dm[0] -= h
+    _, Fp, _ = converged(m, Dp, N, chi)
+    _, Fm, _ = converged(m, Dm, N, chi)
+    fd = (Fp - Fm) / (2 * h)
+    assert abs(dF[0] - fd) <= 1e-4 * max(1.0, abs(fd)), (dF[0], fd)
+    dchi = ctx.dF_dchi(0)
+    _, Fcp, _ = converged(m, D, N, chi + h)
+    _, Fcm, _ = converged(m, D, N, chi - h)
+    fdc = (Fcp - Fcm) / (2 * h)
+    assert abs(dchi - fdc) <= 1e-4 * max(1.0, abs(fdc)), (dchi, fdc)

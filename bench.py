@@ -38,7 +38,26 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="one replica at a time")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--profile-round", type=int, default=0, metavar="R",
+                    help="profiling mode: one batched props round of R replicas of the workload, then exit")
     return ap.parse_args()
+
+
+def profile_round(a, cfg):
+    """One batched props round (prepare, 4 launches per contour step, densities)
+    of the first R replicas of the workload: the unit the ncu captures in
+    profiles/ are taken on."""
+    import scft_string_b200 as S
+    from scft_string_b200.configs import fields
+    c = dict(cfg)
+    c["strn"] = a.profile_round
+    wm, wp = fields(c)
+    ctx = S.StringSolver(c, precision=a.precision, batched=not a.plain)
+    for ii in range(c["strn"]):
+        ctx.set_fields(ii, wm[ii], wp[ii])
+    ctx.solve_field0_all(2, 0.0)
+    print(json.dumps({"profile_round": c["strn"], "precision": a.precision, **ctx.stats()}))
+    return 0
 
 
 def dist_env():
@@ -227,6 +246,8 @@ def main():
     rank, world, dev = dist_env()
     from scft_string_b200.configs import STRING_64
     cfg = dict(STRING_64)
+    if a.profile_round > 0:
+        return profile_round(a, cfg)
     if a.impl == "reference":
         if rank != 0:
             return 0

@@ -148,6 +148,20 @@ scft_status scft_get_box(const scft_ctx *ctx, double *D);
  * stress dF/dL_i = -d lnQ/dL_i, exact at a converged saddle point.  Either
  * output may be NULL. */
 scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL);
+/* Anderson-accelerated solution of replica ii's field equations (an option
+ * beside the reference's simple mixing; no reference counterpart): residual
+ * as scft.cu:605-607 without spring or string terms, history of nhist
+ * (1..30) iterates, FP64 least squares, mixing parameter lam.  Stops when the
+ * RMS residual <= tol; *iters = props evaluations, *err_out = last RMS. */
+scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, int nhist, double lam,
+                                int *iters, double *err_out);
+/* Variable-cell relaxation of replica ii: `inner` iterations of the
+ * solve_field loop on that replica (no FreeE), then a gradient step on the
+ * box, L_i -= gamma dF/dL_i (each relative change capped at 2 %), until
+ * max_i |dF/dL_i| <= stressTol or maxOuter rounds.  *outer_out = rounds run,
+ * stress_out[3] = last dF/dL. */
+scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, double stressTol,
+                            double gamma, int *outer_out, double *stress_out);
 /* dF/d(chi N) of replica ii at a converged saddle point: 1/4 - <W-^2>/chi^2. */
 scft_status scft_dF_dchi(scft_ctx *ctx, int ii, double *out);
 

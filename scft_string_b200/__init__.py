@@ -74,7 +74,8 @@ EXPORTS = [
     "scft_solve_field", "scft_string_begin", "scft_string_step", "scft_string_end",
     "scft_free_energy", "scft_last_free_energy", "scft_spline_derivs", "scft_spline_redist", "scft_get_stats",
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
-    "scft_stress", "scft_dF_dchi",
+    "scft_stress", "scft_dF_dchi", "scft_relax_cell",
+    "scft_anderson_solve",
 ]
 
 _lib = None
@@ -125,6 +126,8 @@ def lib():
     L.scft_get_box.argtypes = [vp, _dp]
     L.scft_stress.argtypes = [vp, C.c_int, _dp, _dp]
     L.scft_dF_dchi.argtypes = [vp, C.c_int, _dp]
+    L.scft_anderson_solve.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
+    L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
     _lib = L
     return L
@@ -325,6 +328,22 @@ class Context:
         a, b = np.zeros(3), np.zeros(3)
         self._ck(lib().scft_stress(self.h, int(ii), _p(a), _p(b)))
         return a, b
+
+    def anderson_solve(self, ii=0, maxIter=2000, tol=1e-10, nhist=10, lam=0.1):
+        """Anderson-mixing solve of replica ii; returns (iterations, RMS residual)."""
+        n = C.c_int()
+        e = C.c_double()
+        self._ck(lib().scft_anderson_solve(self.h, int(ii), int(maxIter), float(tol), int(nhist), float(lam),
+                                           C.byref(n), C.byref(e)))
+        return n.value, e.value
+
+    def relax_cell(self, ii=0, maxOuter=50, inner=20, stressTol=1e-6, gamma=1.0):
+        """Variable-cell relaxation; returns (rounds, last dF/dL, box)."""
+        n = C.c_int()
+        st = np.zeros(3)
+        self._ck(lib().scft_relax_cell(self.h, int(ii), int(maxOuter), int(inner), float(stressTol),
+                                       float(gamma), C.byref(n), _p(st)))
+        return n.value, st, self.get_box()
 
     def dF_dchi(self, ii=0):
         v = C.c_double()

@@ -304,3 +304,59 @@ void launch_reduce_final(const double *partials, int nrows, int nblk, double *ou
 }
 
 }  // namespace scft
+
+// ------------------------------------------------------------------ Anderson mixing
+// (no reference code; the reference keeps only scaffolding for it, scft.cu:30-31)
+namespace scft {
+namespace {
+
+// partial sums of <d_k, d_j> for the n history slots listed in `slots`
+__global__ void k_hist_dots(const double *Dh, size_t n2M, int k, SmallVec slots, double *partials)
+{
+    __shared__ double sh[32];
+    const int j = blockIdx.y;
+    const double *a = Dh + (size_t)k * n2M, *b = Dh + (size_t)(int)slots.v[j] * n2M;
+    double s = 0;
+    for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n2M; r += (size_t)gridDim.x * blockDim.x)
+        s += a[r] * b[r];
+    put_partial(partials, j, s, sh);
+}
+
+// W = (x_k + lam d_k) - sum_i theta_i ((x_k + lam d_k) - (x_i + lam d_i))
+__global__ void k_anderson_update(double *W, const double *Xh, const double *Dh, size_t n2M, int k, int m,
+                                  SmallVec slots, SmallVec theta, double lam)
+{
+    const double *xk = Xh + (size_t)k * n2M, *dk = Dh + (size_t)k * n2M;
+    for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n2M; r += (size_t)gridDim.x * blockDim.x) {
+        const double yk = xk[r] + lam * dk[r];
+        double v = yk;
+        for (int i = 0; i < m; i++) {
+            const size_t o = (size_t)(int)slots.v[i] * n2M + r;
+            v -= theta.v[i] * (yk - (Xh[o] + lam * Dh[o]));
+        }
+        W[r] = v;
+    }
+}
+
+}  // namespace
+
+void launch_hist_dots(const double *Dh, size_t n2M, int k, const int *slots, int n, int nblk, double *partials,
+                      cudaStream_t st)
+{
+    SmallVec sv;
+    for (int i = 0; i < kMaxStrn; i++) sv.v[i] = i < n ? slots[i] : 0;
+    k_hist_dots<<<dim3(nblk, n), kThreads, 0, st>>>(Dh, n2M, k, sv, partials);
+}
+
+void launch_anderson_update(double *W, const double *Xh, const double *Dh, size_t n2M, int k, int m,
+                            const int *slots, const double *theta, double lam, cudaStream_t st)
+{
+    SmallVec sv, th;
+    for (int i = 0; i < kMaxStrn; i++) {
+        sv.v[i] = i < m ? slots[i] : 0;
+        th.v[i] = i < m ? theta[i] : 0;
+    }
+    k_anderson_update<<<512, kThreads, 0, st>>>(W, Xh, Dh, n2M, k, m, sv, th, lam);
+}
+
+}  // namespace scft

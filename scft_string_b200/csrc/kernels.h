@@ -138,5 +138,9 @@ void launch_redist(const FieldArgs &a, const SplineKnots *knots, double lambda, 
 void launch_freee(const FieldArgs &a, int nrep_launch, double f, int nblk, cudaStream_t st);
 void launch_reduce_final(const double *partials, int nrows, int nblk, double *out,
                          cudaStream_t st);
+void launch_hist_dots(const double *Dh, size_t n2M, int k, const int *slots, int n, int nblk, double *partials,
+                      cudaStream_t st);
+void launch_anderson_update(double *W, const double *Xh, const double *Dh, size_t n2M, int k, int m,
+                            const int *slots, const double *theta, double lam, cudaStream_t st);
 
 }  // namespace scft

@@ -82,6 +82,8 @@ struct scft_ctx {
     CUtensorMap tmap;  // spectra as a 2-D array for the x-pencil tiles
     // adjoint (stress) scratch, allocated on first use
     void *st_S4 = nullptr, *st_S2 = nullptr, *st_S4p = nullptr;
+    double *and_X = nullptr, *and_D = nullptr;  // Anderson histories
+    int and_H = 0;
     double *st_part = nullptr, *st_out = nullptr;
     int rt_slab_threads = 0, rt_slab_smem = 0, rt_pencil_threads = 0, rt_pencil_smem = 0;
 
@@ -103,6 +105,7 @@ struct scft_ctx {
         int doii = -1, maxIter = 0, k = 0;
         double errTol = 1e-3, lambda = 0.05, err = 1, errt = 1, FE = 0;
         int dospring = 1, doredist = 0, doperp = 0;
+        bool skip_freee = false;  // cell relaxation runs the loop without FreeE
         std::vector<double> x, xref, alf, errs, errs3, FEs, FEs0, FEs1, phctot;
         std::vector<int> steps;
     } sf;
@@ -491,7 +494,7 @@ void scft_destroy(scft_ctx *ctx)
     void *ptrs[] = {ctx->W, ctx->conc, ctx->DEV, ctx->dWda, ctx->rs, ctx->partials, ctx->redout,
                     ctx->rep_dev, ctx->err, ctx->etab, ctx->hist, ctx->spec, ctx->pbuf, ctx->tw,
                     ctx->kfac, ctx->knots, ctx->st_S4, ctx->st_S2, ctx->st_S4p, ctx->st_part,
-                    ctx->st_out};
+                    ctx->st_out, ctx->and_X, ctx->and_D};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : ctx->tev)
@@ -862,6 +865,7 @@ scft_status scft_string_begin(scft_ctx *ctx, int doii, int maxIter, double errTo
     S.dospring = 1;
     S.doredist = 0;
     S.doperp = 0;
+    S.skip_freee = false;
     if (doii > -1 || ctx->p.dostring != 1) S.dospring = S.doredist = S.doperp = 0;
     if (ctx->p.fix[0] == 1) ctx->doiis[0] = 0;  // scft.cu:587-588
     if (ctx->p.fix[1] == 1) ctx->doiis[ctx->strn - 1] = 0;
@@ -1017,7 +1021,7 @@ scft_status scft_string_step(scft_ctx *ctx, scft_iter_report *rep, double *errs_
     for (int ii = 0; ii < strn; ii++) errtot += S.errs3[ii] * S.errs3[ii] / strn;
     errtot = std::sqrt(errtot);
     int did_fe = 0;
-    if (k % skip == 0 || k == S.maxIter - 1 || !(S.err > S.errTol)) {
+    if (!S.skip_freee && (k % skip == 0 || k == S.maxIter - 1 || !(S.err > S.errTol))) {
         s = free_energy(ctx, &S.FE);
         if (s != SCFT_OK) return s;
         did_fe = 1;
@@ -1267,6 +1271,151 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
         if (dlnQ_dL) dlnQ_dL[i] = d;
         if (dF_dL) dF_dL[i] = -d;
     }
+    return SCFT_OK;
+}
+
+// Anderson-accelerated solution of replica ii's field equations (no
+// reference counterpart; the reference keeps only its scaffolding,
+// scft.cu:30-31): residual d = (chi (phiB - phiA) - 2 W-, chi (phiA + phiB - 1))
+// as in scft.cu:605-607, history of up to nhist previous (W, d), least squares
+// in FP64 on the host over the device-computed Gram matrix of the residuals,
+// W <- (W_k + lam d_k) - sum_i theta_i ((W_k + lam d_k) - (W_i + lam d_i)).
+scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, int nhist, double lam,
+                                int *iters, double *err_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || maxIter < 1 || nhist < 1 || nhist > 30 || !(lam > 0))
+        return SCFT_BAD_INPUT;
+    const size_t n2M = 2 * (size_t)ctx->M;
+    const int H = nhist + 1;
+    if (ctx->and_H < H) {
+        if (ctx->and_X) cudaFree(ctx->and_X);
+        if (ctx->and_D) cudaFree(ctx->and_D);
+        ctx->and_X = ctx->and_D = nullptr;
+        CK(cudaMalloc(&ctx->and_X, sizeof(double) * n2M * H));
+        CK(cudaMalloc(&ctx->and_D, sizeof(double) * n2M * H));
+        ctx->and_H = H;
+    }
+    std::vector<double> G((size_t)H * H, 0.0);
+    std::vector<int> hist;  // slots of previous iterates, most recent first
+    double err = 0;
+    int it = 0;
+    scft_status s;
+    for (; it < maxIter; it++) {
+        s = props_list(ctx, {ii});
+        if (s != SCFT_OK) return s;
+        s = upload_list(ctx, {ii});
+        if (s != SCFT_OK) return s;
+        launch_dev(field_args(ctx, ctx->rep_dev), 1, kRedBlocks, 0, 0.0, ctx->st);
+        s = reduce_rows(ctx, 2, kRedBlocks);
+        if (s != SCFT_OK) return s;
+        err = std::sqrt(ctx->red_h[0] / (double)n2M);
+        if (!(err == err)) {
+            ctx->lasterr = "anderson: residual is NaN";
+            return SCFT_NAN_DETECTED;
+        }
+        if (err <= tol) break;
+        const int k = it % H;
+        double *W = ctx->W + (size_t)ii * n2M;
+        CK(cudaMemcpyAsync(ctx->and_X + (size_t)k * n2M, W, sizeof(double) * n2M, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->and_D + (size_t)k * n2M, ctx->DEV + (size_t)ii * n2M, sizeof(double) * n2M,
+                           cudaMemcpyDeviceToDevice, ctx->st));
+        hist.erase(std::remove(hist.begin(), hist.end(), k), hist.end());
+        if ((int)hist.size() > nhist) hist.resize(nhist);
+        std::vector<int> dslots(1, k);
+        dslots.insert(dslots.end(), hist.begin(), hist.end());
+        launch_hist_dots(ctx->and_D, n2M, k, dslots.data(), (int)dslots.size(), kRedBlocks, ctx->partials, ctx->st);
+        s = reduce_rows(ctx, (int)dslots.size(), kRedBlocks);
+        if (s != SCFT_OK) return s;
+        for (size_t j = 0; j < dslots.size(); j++) G[(size_t)k * H + dslots[j]] = G[(size_t)dslots[j] * H + k] = ctx->red_h[j];
+        const int m = (int)hist.size();
+        std::vector<double> theta(m, 0.0);
+        if (m > 0) {
+            // U theta = v, U_ij = <d_k - d_i, d_k - d_j>, v_i = <d_k, d_k - d_i>
+            std::vector<double> U((size_t)m * m), v(m);
+            const double gkk = G[(size_t)k * H + k];
+            for (int a = 0; a < m; a++) {
+                const int ia = hist[a];
+                v[a] = gkk - G[(size_t)k * H + ia];
+                for (int b = 0; b < m; b++) {
+                    const int ib = hist[b];
+                    U[(size_t)a * m + b] = gkk - G[(size_t)k * H + ia] - G[(size_t)k * H + ib] + G[(size_t)ia * H + ib];
+                }
+            }
+            double tr = 0;
+            for (int a = 0; a < m; a++) tr += U[(size_t)a * m + a];
+            for (int a = 0; a < m; a++) U[(size_t)a * m + a] += 1e-12 * tr + 1e-300;
+            // Gaussian elimination with partial pivoting
+            for (int c = 0; c < m; c++) {
+                int piv = c;
+                for (int r = c + 1; r < m; r++)
+                    if (std::fabs(U[(size_t)r * m + c]) > std::fabs(U[(size_t)piv * m + c])) piv = r;
+                if (piv != c) {
+                    for (int j = 0; j < m; j++) std::swap(U[(size_t)c * m + j], U[(size_t)piv * m + j]);
+                    std::swap(v[c], v[piv]);
+                }
+                for (int r = c + 1; r < m; r++) {
+                    const double fct = U[(size_t)r * m + c] / U[(size_t)c * m + c];
+                    for (int j = c; j < m; j++) U[(size_t)r * m + j] -= fct * U[(size_t)c * m + j];
+                    v[r] -= fct * v[c];
+                }
+            }
+            for (int r = m - 1; r >= 0; r--) {
+                double t = v[r];
+                for (int j = r + 1; j < m; j++) t -= U[(size_t)r * m + j] * theta[j];
+                theta[r] = t / U[(size_t)r * m + r];
+            }
+        }
+        launch_anderson_update(W, ctx->and_X, ctx->and_D, n2M, k, m, hist.data(), theta.data(), lam, ctx->st);
+        ctx->stats.kernel_launches += 2;
+        CK(cudaGetLastError());
+        hist.insert(hist.begin(), k);
+        if ((int)hist.size() > nhist) hist.resize(nhist);
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    if (iters) *iters = it;
+    if (err_out) *err_out = err;
+    return SCFT_OK;
+}
+
+// Variable-cell relaxation of replica ii: `inner` SCFT iterations (the
+// solve_field loop restricted to this replica, scft.cu:598-608, without the
+// periodic FreeE), then L_i -= gamma dF/dL_i with each relative change capped
+// at 2 %, until max |dF/dL_i| <= stressTol.
+scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, double stressTol, double gamma,
+                            int *outer_out, double *stress_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || inner < 1 || maxOuter < 1 || !(gamma > 0)) return SCFT_BAD_INPUT;
+    double dF[3] = {0, 0, 0};
+    int outer = 0;
+    scft_status s = SCFT_OK;
+    for (; outer < maxOuter; outer++) {
+        s = scft_string_begin(ctx, ii, inner, 1e-3);
+        if (s != SCFT_OK) return s;
+        ctx->sf.skip_freee = true;
+        for (int k = 0; k < inner; k++) {
+            int done = 0;
+            s = scft_string_step(ctx, nullptr, nullptr, nullptr, &done);
+            if (s != SCFT_OK) return s;
+            if (done) break;
+        }
+        scft_string_end(ctx, nullptr);
+        s = scft_stress(ctx, ii, nullptr, dF);
+        if (s != SCFT_OK) return s;
+        const double mx = std::max(std::fabs(dF[0]), std::max(std::fabs(dF[1]), std::fabs(dF[2])));
+        if (mx <= stressTol) break;
+        double D[3];
+        for (int i = 0; i < 3; i++) {
+            double step = -gamma * dF[i];
+            const double cap = 0.02 * ctx->p.D[i];
+            step = std::max(-cap, std::min(cap, step));
+            D[i] = ctx->p.D[i] + step;
+        }
+        s = scft_set_box(ctx, D);
+        if (s != SCFT_OK) return s;
+    }
+    if (outer_out) *outer_out = outer;
+    if (stress_out)
+        for (int i = 0; i < 3; i++) stress_out[i] = dF[i];
     return SCFT_OK;
 }
 

@@ -53,13 +53,13 @@ def test_adjoint_matches_finite_differences(built_lib, m, D, N, ens):
     assert np.allclose(d32, dlnq, rtol=2e-4, atol=2e-6)
 
 
-def converged(m, D, N, chi, iters=400):
+def converged(m, D, N, chi):
+    """Saddle point to RMS residual 1e-11 by Anderson mixing."""
     ctx = S.Context(m, D, N, chi=chi, f=0.5, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0)
     wm, wp = smooth_fields(m, D, 2, amp=0.3 * chi)
     ctx.set_fields(0, wm, wp)
-    ctx.solve_field0_all(5000, 1e-10)
-    k, recs, _, _ = ctx.solve_field(iters, errTol=1e-3)
-    ctx.solve_field0(0, 5000, 1e-12)
+    ctx.solve_field(40, errTol=1e-3)
+    n, err = ctx.anderson_solve(0, maxIter=3000, tol=1e-11, nhist=12, lam=0.1)
     ctx.props(0)
     conc, lnQ, _ = ctx.get_conc(0)
     W = ctx.get_fields(0)
@@ -67,14 +67,14 @@ def converged(m, D, N, chi, iters=400):
     pA, pB = conc[:M], conc[M:2 * M]
     wa, wb = W[:M] + W[M:], W[M:] - W[:M]
     F = -lnQ + np.mean(chi * pA * pB - wa * pA - wb * pB)
-    return ctx, F, recs[-1]["errtot"]
+    return ctx, F, err
 
 
 def test_saddle_point_stress_and_dchi(built_lib):
     m, N, chi = (16, 16, 16), 20, 12.0
     D = np.array([3.6, 3.6, 3.6])
     ctx, F0, err = converged(m, D, N, chi)
-    assert err < 1e-7
+    assert err <= 1e-11
     _, dF = ctx.stress(0)
     h = 1e-3
     Dp, Dm = D.copy(), D.copy()
@@ -89,3 +89,21 @@ def test_saddle_point_stress_and_dchi(built_lib):
     _, Fcm, _ = converged(m, D, N, chi - h)
     fdc = (Fcp - Fcm) / (2 * h)
     assert abs(dchi - fdc) <= 1e-4 * max(1.0, abs(fdc)), (dchi, fdc)
+
+
+def test_variable_cell_relaxation_lowers_stress(built_lib):
+    """A lamellar replica in a box longer than its period relaxes its cell:
+    the adjoint stress falls below 1e-6 and the free energy does not rise."""
+    m, N, chi = (8, 8, 24), 20, 14.0
+    D = np.array([2.0, 2.0, 4.6])
+    ctx = S.Context(m, D, N, chi=chi, f=0.5, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0)
+    z = np.arange(m[2]) * D[2] / m[2]
+    wm = np.broadcast_to(0.4 * chi * np.cos(2 * np.pi * z / D[2]), m).ravel()
+    ctx.set_fields(0, wm, np.zeros_like(wm))
+    ctx.solve_field0_all(5000, 1e-8)
+    ctx.solve_field(150)
+    _, s0 = ctx.stress(0)
+    n, st, box = ctx.relax_cell(0, maxOuter=200, inner=15, stressTol=1e-6, gamma=2.0)
+    print("rounds", n, "stress", st, "box", box, "initial stress", s0)
+    assert np.abs(st).max() <= 1e-6
+    assert abs(box[0] - D[0]) < 1e-12 and abs(box[1] - D[1]) < 1e-12  # no x, y structure: no stress

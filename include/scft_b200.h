@@ -175,6 +175,22 @@ scft_status scft_spline_derivs(scft_ctx *ctx, const double *x, const double *con
 scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xref,
                                double *const *ww, int r0, int n, const int *doiis, double lambda);
 
+/* ---- allocation-free step (no counterpart in the reference) ------------ */
+/* One Richardson contour step for callers that cannot allocate device memory
+ * when they need it (a host recording work for later replay, a real-time loop
+ * that must not stall on the allocator, a framework that owns every device
+ * allocation).  Same kernels and result as scft_do_step, but every working
+ * buffer lives in one static __device__ array of 4.2 MB, so it calls no
+ * cudaMalloc/cudaFree.  All pointers are the caller's device memory: w2M =
+ * [W-, W+], in2M = [q(s), q^dagger(s)], out2M = [q(s+1), q^dagger(s+1)], each
+ * 2*M doubles; f is the A fraction as in scft_problem; stream may be NULL.
+ * Limits: FP64, M <= 32768, each m_i <= 64 (BAD_INPUT beyond).  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress): make
+ * it before any stream capture.  Calls share the array, so calls that overlap
+ * on the GPU race; the call waits for its stream before returning. */
+scft_status scft_do_step_noalloc(const int *m, const double *D, int N, double f, const double *w2M,
+                                 const double *in2M, double *out2M, int s, void *stream);
+
 /* ---- statistics ------------------------------------------------------- */
 /* Records CUDA event `slot` (0..3) on the context's stream; elapsed device
  * time between two recorded slots (waits for the later one). */

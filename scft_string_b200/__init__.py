@@ -74,7 +74,7 @@ EXPORTS = [
     "scft_solve_field", "scft_string_begin", "scft_string_step", "scft_string_end",
     "scft_free_energy", "scft_last_free_energy", "scft_spline_derivs", "scft_spline_redist", "scft_get_stats",
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
-    "scft_stress", "scft_dF_dchi", "scft_relax_cell",
+    "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve",
 ]
 
@@ -126,6 +126,8 @@ def lib():
     L.scft_get_box.argtypes = [vp, _dp]
     L.scft_stress.argtypes = [vp, C.c_int, _dp, _dp]
     L.scft_dF_dchi.argtypes = [vp, C.c_int, _dp]
+    L.scft_do_step_noalloc.argtypes = [_ip, _dp, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.c_void_p]
     L.scft_anderson_solve.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
     L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]

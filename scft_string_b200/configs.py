@@ -75,3 +75,32 @@ def win_text(wm_row, wp_row) -> str:
     """A ``win`` file with full double precision (read back exactly by
     ``fscanf("%lf %lf")`` in the reference, scft.cu:1062)."""
     return "".join(f"{a:.17g} {b:.17g}\n" for a, b in zip(wm_row, wp_row))
+
+
+def uneven_batch(seed: int = 5):
+    """The 24 independent solves of the uneven-batch workload: 8 at 48^3, 10
+    at 64^3 and 6 at 96^3 (D = m/16), with N drawn from {64, 96, 128, 192,
+    256}, chiN from U[12, 25], f from U[0.3, 0.5] and phidb from U[0.6, 1.0]
+    by default_rng(seed) in that order per solve, and W- = Gaussian noise
+    0.1*chiN from default_rng([seed, j]).  ens = 2 (the reference default):
+    in the canonical ensemble alpha*N = 6.4 ... 25.6 is never an integer and
+    the W+ relaxation cannot converge (see the notes on Nh)."""
+    rng = np.random.default_rng(seed)
+    grids = [48] * 8 + [64] * 10 + [96] * 6
+    out = []
+    for j, mm in enumerate(grids):
+        N = int(rng.choice([64, 96, 128, 192, 256]))
+        chi = float(rng.uniform(12, 25))
+        f = float(rng.uniform(0.3, 0.5))
+        phidb = float(rng.uniform(0.6, 1.0))
+        out.append(dict(name=f"solve{j}_{mm}cubed_N{N}", chi=chi, f=f, ens=2, phidb=phidb, N=N, alpha=0.1,
+                        m=(mm, mm, mm), D=(mm / 16.0,) * 3, fix=(0, 0), dostring=0, strn=1,
+                        noise_seed=[seed, j]))
+    return out
+
+
+def noise_fields(c: dict):
+    """W- = N(0, 0.1*chiN) from default_rng(c['noise_seed']), W+ = 0."""
+    M = int(np.prod(c["m"]))
+    wm = np.random.default_rng(c["noise_seed"]).normal(0.0, 0.1 * c["chi"], M)
+    return wm, np.zeros(M)

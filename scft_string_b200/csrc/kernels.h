@@ -40,6 +40,7 @@ struct PropsArgs {
     double chi, phic, alpha;
     int ens;
     int *err;               // device error word (launch-geometry / plan errors)
+    int slot0;              // first slot of this launch within the spectra tensor map
 };
 
 struct PropsLaunch {

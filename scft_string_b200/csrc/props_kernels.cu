@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const int ncol = m1 * mk2, c0 = tile * TC;
     const int x = 2 * c0;
-    const int y0 = ((slot * 2 + fld) * 2) * m0;
+    const int y0 = (((a.slot0 + slot) * 2 + fld) * 2) * m0;
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);

@@ -65,8 +65,9 @@ struct scft_ctx {
     Geo g;
     int M, Mk, strn, nrep_alloc, nslots, prec;
     double f;  // rounded A fraction
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
+    int ngroups = 2;
     cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
     PropsLaunch L;
     std::string lasterr;
@@ -149,6 +150,23 @@ PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
     a.alpha = ctx->p.alpha;
     a.ens = ctx->p.ens;
     a.err = ctx->err;
+    a.slot0 = 0;
+    return a;
+}
+
+// the same arguments for the slots [s0, s0 + n) of a round: every per-slot
+// base pointer moves by s0 slots
+template <typename T>
+PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0)
+{
+    PropsArgs<T> a = props_args<T>(ctx, slot_rep + s0);
+    const size_t M = ctx->M, Mk = ctx->Mk;
+    a.etab += (size_t)s0 * 2 * M;
+    a.hist += (size_t)s0 * (ctx->g.Ns + 1) * 2 * M;
+    a.spec += (size_t)s0 * 2 * 2 * Mk;
+    a.pbuf += (size_t)s0 * 2 * M;
+    a.partials += (size_t)s0 * ctx->npart_stride;
+    a.slot0 = s0;
     return a;
 }
 
@@ -197,10 +215,28 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
     int launches = 0;
     for (size_t c0 = 0; c0 < reps.size(); c0 += ctx->nslots) {
         const int nb = (int)std::min<size_t>(ctx->nslots, reps.size() - c0);
+        // groups of slots run as independent chains on two streams, so the
+        // last wave of one group's launch overlaps the other group's work
+        const int ng = (ctx->ngroups > 1 && nb >= 2 * ctx->ngroups) ? ctx->ngroups : 1;
         auto launch = [&]() {
-            if (ctx->prec == SCFT_FP32)
-                return launch_props<float>(props_args<float>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
-            return launch_props<double>(props_args<double>(ctx, ctx->rep_dev + c0), ctx->L, nb, ctx->st);
+            int n = 0;
+            if (ng > 1) {
+                cudaEventRecord(ctx->fork, ctx->st);
+                cudaStreamWaitEvent(ctx->st2, ctx->fork, 0);
+            }
+            for (int gi = 0; gi < ng; gi++) {
+                const int s0 = nb * gi / ng, s1 = nb * (gi + 1) / ng;
+                cudaStream_t sg = (gi % 2 == 0) ? ctx->st : ctx->st2;
+                if (ctx->prec == SCFT_FP32)
+                    n += launch_props<float>(props_args_from<float>(ctx, ctx->rep_dev + c0, s0), ctx->L, s1 - s0, sg);
+                else
+                    n += launch_props<double>(props_args_from<double>(ctx, ctx->rep_dev + c0, s0), ctx->L, s1 - s0, sg);
+            }
+            if (ng > 1) {
+                cudaEventRecord(ctx->join, ctx->st2);
+                cudaStreamWaitEvent(ctx->st, ctx->join, 0);
+            }
+            return n;
         };
         const size_t key = (c0 <= (size_t)ctx->nrep_alloc) ? c0 * (ctx->nslots + 1) + nb : (size_t)-1;
         if (ctx->use_graphs && key < ctx->graphs.size()) {
@@ -215,7 +251,7 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
                 if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
             }
             CK(cudaGraphLaunch(ctx->graphs[key], ctx->st));
-            launches += 4 * ctx->g.Ns + 6;
+            launches += (4 * ctx->g.Ns + 6) * ng;
         } else {
             launches += launch();
         }
@@ -501,6 +537,9 @@ void scft_destroy(scft_ctx *ctx)
         if (e) cudaEventDestroy(e);
     for (auto &g : ctx->graphs)
         if (g) cudaGraphExecDestroy(g);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
+    if (ctx->st2) cudaStreamDestroy(ctx->st2);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -608,6 +647,10 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         ctx->npart_stride = 6 * kRedBlocks;
         ctx->nred_rows = 2 * kMaxStrn + 8;
         CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+        CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+        CKC(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+        CKC(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
+        if (const char *ev = getenv("SCFT_GROUPS")) ctx->ngroups = std::max(1, std::min(2, atoi(ev)));
         CKC(cudaEventCreate(&ctx->ev0));
         CKC(cudaEventCreate(&ctx->ev1));
         for (auto &e : ctx->tev) CKC(cudaEventCreate(&e));

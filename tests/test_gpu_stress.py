@@ -53,13 +53,14 @@ def test_adjoint_matches_finite_differences(built_lib, m, D, N, ens):
     assert np.allclose(d32, dlnq, rtol=2e-4, atol=2e-6)
 
 
-def converged(m, D, N, chi):
-    """Saddle point to RMS residual 1e-11 by Anderson mixing."""
+def converged(D, chi, m=(8, 8, 24), N=20):
+    """Lamellar saddle point (z structure) to RMS residual 1e-10 by Anderson mixing."""
+    D = np.asarray(D, float)
     ctx = S.Context(m, D, N, chi=chi, f=0.5, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0)
-    wm, wp = smooth_fields(m, D, 2, amp=0.3 * chi)
-    ctx.set_fields(0, wm, wp)
-    ctx.solve_field(40, errTol=1e-3)
-    n, err = ctx.anderson_solve(0, maxIter=3000, tol=1e-11, nhist=12, lam=0.1)
+    z = np.arange(m[2]) * D[2] / m[2]
+    wm = np.broadcast_to(0.4 * chi * np.cos(2 * np.pi * z / D[2]), m).ravel()
+    ctx.set_fields(0, wm, np.zeros_like(wm))
+    n, err = ctx.anderson_solve(0, maxIter=2000, tol=1e-10, nhist=12, lam=0.1)
     ctx.props(0)
     conc, lnQ, _ = ctx.get_conc(0)
     W = ctx.get_fields(0)
@@ -71,24 +72,27 @@ def converged(m, D, N, chi):
 
 
 def test_saddle_point_stress_and_dchi(built_lib):
-    m, N, chi = (16, 16, 16), 20, 12.0
-    D = np.array([3.6, 3.6, 3.6])
-    ctx, F0, err = converged(m, D, N, chi)
-    assert err <= 1e-11
+    """At a converged saddle point the adjoint stress dF/dLz and the closed
+    form dF/dchiN match central differences of re-converged free energies."""
+    chi = 14.0
+    D = np.array([2.0, 2.0, 4.6])
+    ctx, F0, err = converged(D, chi)
+    assert err <= 1e-10
     _, dF = ctx.stress(0)
+    assert abs(dF[0]) < 1e-12 and abs(dF[1]) < 1e-12  # no x, y structure
     h = 1e-3
-    Dp, Dm = D.copy(), D.copy()
-    Dp[0] += h
-    Dm[0] -= h
-    _, Fp, _ = converged(m, Dp, N, chi)
-    _, Fm, _ = converged(m, Dm, N, chi)
+    _, Fp, ep = converged(D + [0, 0, h], chi)
+    _, Fm, em = converged(D - [0, 0, h], chi)
+    assert max(ep, em) <= 1e-10
     fd = (Fp - Fm) / (2 * h)
-    assert abs(dF[0] - fd) <= 1e-4 * max(1.0, abs(fd)), (dF[0], fd)
+    print("dF/dLz adjoint", dF[2], "fd", fd)
+    assert abs(dF[2] - fd) <= 1e-6 * max(1.0, abs(fd)) + 1e-9
     dchi = ctx.dF_dchi(0)
-    _, Fcp, _ = converged(m, D, N, chi + h)
-    _, Fcm, _ = converged(m, D, N, chi - h)
+    _, Fcp, _ = converged(D, chi + h)
+    _, Fcm, _ = converged(D, chi - h)
     fdc = (Fcp - Fcm) / (2 * h)
-    assert abs(dchi - fdc) <= 1e-4 * max(1.0, abs(fdc)), (dchi, fdc)
+    print("dF/dchi closed form", dchi, "fd", fdc)
+    assert abs(dchi - fdc) <= 1e-6 * max(1.0, abs(fdc))
 
 
 def test_variable_cell_relaxation_lowers_stress(built_lib):

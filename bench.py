@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="one replica at a time")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="string", choices=["string", "uneven24"],
+    ap.add_argument("--workload", default="string", choices=["string", "uneven24", "mixed128", "adjoint96"],
                     help="uneven24: the 24 independent solves of mixed grids and N, run concurrently")
     ap.add_argument("--tol", type=float, default=1e-5, help="uneven24: RMS residual target")
     ap.add_argument("--serial-fp64", action="store_true",
@@ -217,6 +217,132 @@ def run_uneven(a):
     return 0
 
 
+def f_per_chain(ctx, c, W):
+    """props at fields W (2M) of replica 0 and F = -lnQ + <chi pA pB - wA pA - wB pB>."""
+    import numpy as np
+    M = ctx.M
+    ctx.set_fields_2m(0, np.ascontiguousarray(W))
+    ctx.props(0)
+    conc, lnQ, _ = ctx.get_conc(0)
+    pA, pB = conc[:M], conc[M:2 * M]
+    wa, wb = W[:M] + W[M:], W[M:] - W[:M]
+    return -lnQ + np.mean(c["chi"] * pA * pB - wa * pA - wb * pB), lnQ, pA
+
+
+def run_mixed128(a):
+    """128^3, N=200, 8 replicas: FP64 and FP32 from the same start; errors of the
+    FP32 path at identical fields (lnQ, F, rhoA, errtot) and both throughputs."""
+    import numpy as np
+    import torch
+
+    import scft_string_b200 as S
+    from scft_string_b200.configs import MIXED_128, gyroid_fields
+    torch.cuda.set_device(0)
+    c = dict(MIXED_128)
+    wm, wp = gyroid_fields(c)
+    out = {"workload": c["name"]}
+    W64 = None
+    for prec in ("fp64", "fp32"):
+        ctx = S.StringSolver(c, precision=prec, batched=True)
+        for ii in range(c["strn"]):
+            ctx.set_fields(ii, wm[ii], wp[ii])
+        ctx.solve_field0_all(30, 0.0)
+        ctx.string_begin(4000, 1e-3)
+        ctx.string_step()  # k = 0 carries FreeE
+        ctx.reset_stats()
+        ctx.timer_mark(0)
+        reps = [ctx.string_step() for _ in range(a.steps)]
+        ctx.timer_mark(1)
+        st = ctx.stats()
+        out[prec] = {"iters_per_s": a.steps / (ctx.timer_elapsed_ms(0, 1) / 1e3),
+                     "contour_steps_per_s": st["contour_steps"] / st["props_seconds"],
+                     "errtot": [r["errtot"] for r in reps]}
+        if prec == "fp64":
+            W64 = [ctx.get_fields(ii) for ii in range(c["strn"])]
+        ctx.close()
+    # FP32 errors at the FP64 fields, replica by replica
+    dF, dQ, drho = [], [], []
+    one64 = S.StringSolver(dict(c, strn=1), precision="fp64")
+    one32 = S.StringSolver(dict(c, strn=1), precision="fp32")
+    for W in W64:
+        F64, q64, r64 = f_per_chain(one64, c, W)
+        F32, q32, r32 = f_per_chain(one32, c, W)
+        dF.append(abs(F32 - F64))
+        dQ.append(abs(q32 - q64) / abs(q64))
+        drho.append(float(np.abs(r32 - r64).max()))
+    e64 = np.array(out["fp64"]["errtot"])
+    e32 = np.array(out["fp32"]["errtot"])
+    out["fp32_error"] = {"F_per_chain_max": max(dF), "lnQ_rel_max": max(dQ), "rhoA_maxabs": max(drho),
+                         "errtot_rel_max": float(np.max(np.abs(e32 - e64) / e64))}
+    out["fp32_speedup"] = out["fp32"]["contour_steps_per_s"] / out["fp64"]["contour_steps_per_s"]
+    print(json.dumps(out))
+    return 0
+
+
+def run_adjoint96(a):
+    """64x64x96, N=160 single replica: converged saddle point (Anderson), box
+    stress from the FP64 and FP32 adjoints against central differences of
+    re-converged FP64 free energies (h = 1e-4), dF/dchiN likewise, then
+    variable-cell relaxation to |stress| <= 1e-6."""
+    import numpy as np
+    import torch
+
+    import scft_string_b200 as S
+    from scft_string_b200.configs import ADJOINT_96, hex_fields
+    torch.cuda.set_device(0)
+    c = dict(ADJOINT_96)
+    wm, wp = hex_fields(c)
+    t0 = time.time()
+
+    def converged(D, chi, prec="fp64", W0=None):
+        cc = dict(c, D=tuple(D), chi=chi)
+        ctx = S.StringSolver(cc, precision=prec)
+        if W0 is None:
+            ctx.set_fields(0, wm[0], wp[0])
+        else:
+            ctx.set_fields_2m(0, np.ascontiguousarray(W0))
+        n, err = ctx.anderson_solve(0, maxIter=3000, tol=1e-9, nhist=12, lam=0.1)
+        F, _, _ = f_per_chain(ctx, cc, ctx.get_fields(0))
+        return ctx, F, err, n
+
+    D0 = np.array(c["D"])
+    ctx, F0, err0, n0 = converged(D0, c["chi"])
+    W = ctx.get_fields(0)
+    _, dF64 = ctx.stress(0)
+    c32 = S.StringSolver(c, precision="fp32")
+    c32.set_fields_2m(0, np.ascontiguousarray(W))
+    _, dF32 = c32.stress(0)
+    c32.close()
+    h = 1e-4
+    fd = []
+    for i in range(3):
+        e = np.zeros(3)
+        e[i] = h
+        cp, Fp, _, _ = converged(D0 + e, c["chi"], W0=W)
+        cp.close()
+        cm, Fm, _, _ = converged(D0 - e, c["chi"], W0=W)
+        cm.close()
+        fd.append((Fp - Fm) / (2 * h))
+    dchi = ctx.dF_dchi(0)
+    cp, Fcp, _, _ = converged(D0, c["chi"] + h, W0=W)
+    cp.close()
+    cm, Fcm, _, _ = converged(D0, c["chi"] - h, W0=W)
+    cm.close()
+    fdc = (Fcp - Fcm) / (2 * h)
+    relax = None
+    if err0 < 1e-7:  # relax from a converged saddle only
+        n, st, box = ctx.relax_cell(0, maxOuter=20, inner=0, stressTol=1e-6, gamma=2.0)
+        relax = {"rounds": n, "final_stress": list(st), "box": list(box)}
+    out = {"workload": c["name"], "saddle_residual": err0, "anderson_iters": n0, "F": F0,
+           "dF_dL_fp64_adjoint": list(dF64), "dF_dL_fp32_adjoint": list(dF32), "dF_dL_fd": fd,
+           "dF_dL_fp32_vs_fp64_rel": float(np.max(np.abs(dF32 - dF64)) / max(1e-30, np.max(np.abs(dF64)))),
+           "dF_dchi_closed_form": dchi, "dF_dchi_fd": fdc,
+           "relax": relax,
+           "checkpointing": "all q slices stored (no sqrt(N) recompute)", "wall_s": time.time() - t0}
+    print(json.dumps(out))
+    return 0
+
+
 def run_ours(a, cfg, rank, world, dev):
     import numpy as np
     import torch
@@ -240,6 +366,7 @@ def run_ours(a, cfg, rank, world, dev):
     ctx = S.StringSolver(cfg, precision=a.precision, batched=not a.plain, device=dev)
     for ii in range(cfg["strn"]):
         ctx.set_fields(ii, wm[ii], wp[ii])
+    groups, tune_ms = ctx.autotune()           # 1 or 2 concurrent slot groups per props round
     ctx.solve_field0_all(5000, 1e-4)           # prelude, scft.cu:1105
     nsterp = 4000                              # scft.cu:1102
     ctx.string_begin(nsterp, 1e-3)
@@ -273,7 +400,8 @@ def run_ours(a, cfg, rank, world, dev):
     ctx.timer_mark(3)
     e2e_ms = max_over_ranks(ctx.timer_elapsed_ms(2, 3))
     barrier()
-    out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M)
+    out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M,
+               schedule={"slot_groups": groups, "props_round_ms_by_groups": tune_ms})
     # ---- plain FP64 path on the same state, same first iterations
     if rank == 0 and world == 1 and not a.no_fp64 and a.precision == "fp32":
         k2 = min(2, a.steps)
@@ -312,6 +440,10 @@ def main():
         return profile_round(a, cfg)
     if a.workload == "uneven24":
         return run_uneven(a) if rank == 0 else 0
+    if a.workload == "mixed128":
+        return run_mixed128(a) if rank == 0 else 0
+    if a.workload == "adjoint96":
+        return run_adjoint96(a) if rank == 0 else 0
     if a.impl == "reference":
         if rank != 0:
             return 0
@@ -366,6 +498,7 @@ def main():
         "config": {"workload": cfg["name"], "replicas": cfg["strn"], "grid": list(cfg["m"]),
                    "N": cfg["N"], "ens": cfg["ens"], "precision": a.precision,
                    "batched": not a.plain, "parallelism": f"replicas-only x{world}",
+                   "schedule": r["schedule"],
                    "window": f"iterations k={a.warmup}..{a.warmup + a.steps - 1} after the W+ prelude",
                    "l2": "inputs larger than L2 (propagator store "
                          f"{cfg['strn'] * (cfg['N'] + 1) * 2 * M * b / 1e9:.1f} GB per props round)"},

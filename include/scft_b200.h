@@ -158,7 +158,8 @@ scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, 
 /* Variable-cell relaxation of replica ii: `inner` iterations of the
  * solve_field loop on that replica (no FreeE), then a gradient step on the
  * box, L_i -= gamma dF/dL_i (each relative change capped at 2 %), until
- * max_i |dF/dL_i| <= stressTol or maxOuter rounds.  *outer_out = rounds run,
+ * max_i |dF/dL_i| <= stressTol or maxOuter rounds; inner <= 0 re-solves the
+ * fields by Anderson mixing (to 1e-9) instead.  *outer_out = rounds run,
  * stress_out[3] = last dF/dL. */
 scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, double stressTol,
                             double gamma, int *outer_out, double *stress_out);
@@ -198,6 +199,14 @@ scft_status scft_timer_mark(scft_ctx *ctx, int slot);
 scft_status scft_timer_elapsed(scft_ctx *ctx, int slot_a, int slot_b, double *ms);
 scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
 scft_status scft_reset_stats(scft_ctx *ctx);
+
+/* Picks the number of concurrent slot groups of a props round (1 or 2) by
+ * timing props rounds of all replicas at their current fields with each
+ * setting; the densities are recomputed, the statistics left unchanged.
+ * *groups_out = the setting kept; times_ms[0..1] = best round time with 1 and
+ * 2 groups (either pointer may be NULL).  Performance-only: results do not
+ * depend on the setting. */
+scft_status scft_autotune(scft_ctx *ctx, int *groups_out, double *times_ms);
 
 #ifdef __cplusplus
 }

@@ -75,7 +75,7 @@ EXPORTS = [
     "scft_free_energy", "scft_last_free_energy", "scft_spline_derivs", "scft_spline_redist", "scft_get_stats",
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
-    "scft_anderson_solve",
+    "scft_anderson_solve", "scft_autotune",
 ]
 
 _lib = None
@@ -131,6 +131,7 @@ def lib():
     L.scft_anderson_solve.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
     L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
+    L.scft_autotune.argtypes = [vp, _ip, _dp]
     _lib = L
     return L
 
@@ -351,6 +352,13 @@ class Context:
         v = C.c_double()
         self._ck(lib().scft_dF_dchi(self.h, int(ii), C.byref(v)))
         return v.value
+
+    def autotune(self):
+        """Slot-group count kept (1 or 2) and the best props-round times in ms for 1 and 2."""
+        g = C.c_int()
+        t = np.zeros(2)
+        self._ck(lib().scft_autotune(self.h, C.byref(g), _p(t)))
+        return g.value, [float(t[0]), float(t[1])]
 
     def timer_mark(self, slot):
         """Records CUDA event `slot` on the context's stream."""

@@ -104,3 +104,43 @@ def noise_fields(c: dict):
     M = int(np.prod(c["m"]))
     wm = np.random.default_rng(c["noise_seed"]).normal(0.0, 0.1 * c["chi"], M)
     return wm, np.zeros(M)
+
+
+# Mixed-precision scaling: 128^3, N=200, 8 independent replicas, grand canonical
+# with fugacity 1.0, gyroid start with per-replica noise (seed 3 + ii).
+MIXED_128 = dict(name="mixed8_128cubed_N200", chi=20.0, f=0.35, ens=2, phidb=1.0, N=200, alpha=0.1,
+                 m=(128, 128, 128), D=(6.4, 6.4, 6.4), fix=(0, 0), dostring=0, strn=8, seed=3)
+
+# Adjoint check: 64x64x96, Lx = Ly = 4.2, Lz = 6.3, N=160, canonical (alpha N = 16,
+# n1 = 64, n2 = 96 all even), hexagonal start with noise (seed 4).
+ADJOINT_96 = dict(name="adjoint_64x64x96_N160", chi=16.0, f=0.4, ens=1, phidb=0.9, N=160, alpha=0.1,
+                  m=(64, 64, 96), D=(4.2, 4.2, 6.3), fix=(0, 0), dostring=0, strn=1, seed=4)
+
+
+def gyroid_fields(c: dict):
+    """W- = 0.4 chiN (sin X cos Y + sin Y cos Z + sin Z cos X) with X = 2 pi x / D,
+    plus noise 0.03 chiN from default_rng(seed + ii) per replica; W+ = 0."""
+    m, D = c["m"], c["D"]
+    ax = [2 * np.pi * np.arange(m[i]) * (D[i] / m[i]) / D[i] for i in range(3)]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    base = (0.4 * c["chi"] * (np.sin(X) * np.cos(Y) + np.sin(Y) * np.cos(Z) + np.sin(Z) * np.cos(X))).ravel()
+    M = base.size
+    wm = np.stack([base + np.random.default_rng(c["seed"] + ii).normal(0, 0.03 * c["chi"], M)
+                   for ii in range(c["strn"])])
+    return wm, np.zeros_like(wm)
+
+
+def hex_fields(c: dict):
+    """W- = 0.5 chiN sum_j cos(G_j . r), three in-plane wave vectors at 120 degrees
+    with |G| = 2 pi / Lx, evaluated on the (square) grid, plus noise 0.02 chiN
+    (default_rng(seed)); W+ = 0."""
+    m, D = c["m"], c["D"]
+    x = [np.arange(m[i]) * D[i] / m[i] for i in range(3)]
+    X, Y, _ = np.meshgrid(*x, indexing="ij")
+    g = 2 * np.pi / D[0]
+    w = np.zeros(m)
+    for j in range(3):
+        a = 2 * np.pi * j / 3
+        w += np.cos(g * (np.cos(a) * X + np.sin(a) * Y))
+    wm = 0.5 * c["chi"] * w.ravel() + np.random.default_rng(c["seed"]).normal(0, 0.02 * c["chi"], w.size)
+    return wm[None, :], np.zeros((1, w.size))

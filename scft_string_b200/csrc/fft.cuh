@@ -395,92 +395,96 @@ __device__ __forceinline__ void fft_fixed(cplx<T> *buf, const cplx<T> *tw, int s
     }
 }
 
+// Packed z-rows of the fixed shapes sit at an odd stride of M2 + 1 complex
+// elements, so that a warp transforming 32 rows at once (lines fastest) reads
+// and writes 32 different banks; the half spectra [y][kz] keep their natural
+// stride MK2.  The two layouts overlap, so the repack goes through registers
+// with a block-wide barrier between the reads and the writes.
+template <int M2>
+struct PackedRows {
+    static constexpr int LSF = M2 + 1;
+};
+
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
 {
-    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, NW = NT / 32, TL = (MK2 + 31) / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-    for (int p = warp; p < NPAIR; p += NW) {
-        cplx<T> *row = buf + 2 * p * MK2;
-        const bool has_b = (2 * p + 1 < M1);
-        cplx<T> A[TL], B[TL];
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
+    constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
+    cplx<T> A[PER], B[PER];
 #pragma unroll
-        for (int t = 0; t < TL; t++) {
-            const int kz = lane + 32 * t;
-            if (kz < MK2) {
-                const cplx<T> ck = row[kz];
-                const cplx<T> cm = row[kz == 0 ? 0 : M2 - kz];
-                A[t] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
-                B[t] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
-            }
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            const cplx<T> ck = buf[p * LS + kz];
+            const cplx<T> cm = buf[p * LS + (kz == 0 ? 0 : M2 - kz)];
+            A[i] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
+            B[i] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
         }
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < TL; t++) {
-            const int kz = lane + 32 * t;
-            if (kz < MK2) {
-                row[kz] = A[t];
-                if (has_b) row[MK2 + kz] = B[t];
-            }
-        }
-        __syncwarp();
     }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            buf[2 * p * MK2 + kz] = A[i];
+            if (2 * p + 1 < M1) buf[(2 * p + 1) * MK2 + kz] = B[i];
+        }
+    }
+    __syncthreads();
 }
 
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
 {
-    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, NW = NT / 32, TL = (MK2 + 31) / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-    for (int p = warp; p < NPAIR; p += NW) {
-        cplx<T> *row = buf + 2 * p * MK2;
-        const bool has_b = (2 * p + 1 < M1);
-        cplx<T> A[TL], B[TL];
+    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
+    constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
+    cplx<T> A[PER], B[PER];
 #pragma unroll
-        for (int t = 0; t < TL; t++) {
-            const int kz = lane + 32 * t;
-            if (kz < MK2) {
-                A[t] = row[kz];
-                B[t] = has_b ? row[MK2 + kz] : cplx<T>{(T)0, (T)0};
-                if (kz == 0 || 2 * kz == M2) {
-                    A[t].y = (T)0;
-                    B[t].y = (T)0;
-                }
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            A[i] = buf[2 * p * MK2 + kz];
+            B[i] = (2 * p + 1 < M1) ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
+            if (kz == 0 || 2 * kz == M2) {
+                A[i].y = (T)0;
+                B[i].y = (T)0;
             }
         }
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < TL; t++) {
-            const int kz = lane + 32 * t;
-            if (kz < MK2) {
-                row[kz] = {A[t].x - B[t].y, A[t].y + B[t].x};
-                if (kz > 0 && 2 * kz < M2) row[M2 - kz] = {A[t].x + B[t].y, B[t].x - A[t].y};
-            }
-        }
-        __syncwarp();
     }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            buf[p * LS + kz] = {A[i].x - B[i].y, A[i].y + B[i].x};
+            if (kz > 0 && 2 * kz < M2) buf[p * LS + M2 - kz] = {A[i].x + B[i].y, B[i].x - A[i].y};
+        }
+    }
+    __syncthreads();
 }
 
+// packed real rows (stride M2 + 1) -> half spectrum [y][kz]
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
 {
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
-    fft_fixed<T, M2, NPAIR, 1, 2 * MK2, false, NT>(buf, twz, -1);
+    fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, -1);
     slab_unpack_fixed<T, M1, M2, NT>(buf);
-    __syncthreads();
     fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, -1);
 }
 
+// half spectrum [y][kz] -> packed real rows (stride M2 + 1, unnormalised)
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
 {
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
     fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, +1);
     slab_pack_fixed<T, M1, M2, NT>(buf);
-    __syncthreads();
-    fft_fixed<T, M2, NPAIR, 1, 2 * MK2, false, NT>(buf, twz, +1);
+    fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, +1);
 }
 
 }  // namespace scft

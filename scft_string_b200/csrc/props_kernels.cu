@@ -61,6 +61,17 @@ __global__ void k_prepare(PropsArgs<T> a)
 }
 
 // ---------------------------------------------------------------- shape dispatch
+// Offset of packed z-row p (real lines 2p, 2p+1) in a slab buffer: stride
+// M2 + 1 for the compile-time shapes, 2 mk2 for the runtime path.
+template <int FM2>
+__device__ __forceinline__ int prow(int p, int mk2)
+{
+    if constexpr (FM2 != 0)
+        return p * PackedRows<FM2>::LSF;
+    else
+        return 2 * p * mk2;
+}
+
 // FM0/FM1/FM2 = 0: sizes from the runtime Geo; otherwise compile-time sizes
 // (blockDim.x == MT, tile width from kTile<T>).
 template <typename T>
@@ -126,7 +137,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
         const T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
         for (int e = threadIdx.x; e < npz; e += nthr) {
             const int p = e / m2, z = e - p * m2;
-            cplx<T> &c = buf[2 * p * mk2 + z];
+            cplx<T> &c = buf[prow<FM2>(p, mk2) + z];
             const int r0 = 2 * p * m2 + z;
             // Richardson, GPU_kernels.h:199-203
             c.x = (c.x * E4[r0] * (T)4 - P[r0]) / (T)3;
@@ -144,7 +155,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
             const int p = e / m2, z = e - p * m2;
             const int r0 = 2 * p * m2 + z;
             const bool hb = 2 * p + 1 < m1;
-            buf[2 * p * mk2 + z] = {(T)1, hb ? (T)1 : (T)0};
+            buf[prow<FM2>(p, mk2) + z] = {(T)1, hb ? (T)1 : (T)0};
             qn[r0] = (T)1;
             if (hb) qn[r0 + m2] = (T)1;
         }
@@ -153,7 +164,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
             const int p = e / m2, z = e - p * m2;
             const int r0 = 2 * p * m2 + z;
             const bool hb = 2 * p + 1 < m1;
-            buf[2 * p * mk2 + z] = {qn[r0], hb ? qn[r0 + m2] : (T)0};
+            buf[prow<FM2>(p, mk2) + z] = {qn[r0], hb ? qn[r0 + m2] : (T)0};
         }
     }
     if (sn >= g.Ns) return;
@@ -162,7 +173,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     // half step input E4' q'
     for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
-        cplx<T> &c = buf[2 * p * mk2 + z];
+        cplx<T> &c = buf[prow<FM2>(p, mk2) + z];
         const int r0 = 2 * p * m2 + z;
         c.x *= E4n[r0];
         if (2 * p + 1 < m1) c.y *= E4n[r0 + m2];
@@ -181,7 +192,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
             const T e1 = E4n[r0 + m2];
             v1 = qn[r0 + m2] * (e1 * e1);
         }
-        buf[2 * p * mk2 + z] = {v0, v1};
+        buf[prow<FM2>(p, mk2) + z] = {v0, v1};
     }
     __syncthreads();
     slab_fwd<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
@@ -219,7 +230,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
     for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
-        const cplx<T> c = buf[2 * p * mk2 + z];
+        const cplx<T> c = buf[prow<FM2>(p, mk2) + z];
         const int r0 = 2 * p * m2 + z;
         const T e0 = E4[r0];
         P[r0] = c.x * (e0 * e0);
@@ -235,7 +246,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
     for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
-        cplx<T> &c = buf[2 * p * mk2 + z];
+        cplx<T> &c = buf[prow<FM2>(p, mk2) + z];
         const int r0 = 2 * p * m2 + z;
         const T e0 = E4[r0];
         c.x *= e0 * e0;
@@ -375,7 +386,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     mbar_wait(&bars[1], 0, a.err);
     for (int e = threadIdx.x; e < npz; e += MT) {
         const int p = e / m2, z = e - p * m2;
-        const cplx<T> c = bufB[2 * p * mk2 + z];
+        const cplx<T> c = bufB[prow<FM2>(p, mk2) + z];
         const int r0 = 2 * p * m2 + z;
         const T e0 = E4s[r0];
         P[r0] = c.x * (e0 * e0);
@@ -389,7 +400,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     slab_inverse_fixed<T, m1, m2, MT>(bufA, twy, twz);
     for (int e = threadIdx.x; e < npz; e += MT) {
         const int p = e / m2, z = e - p * m2;
-        cplx<T> &c = bufA[2 * p * mk2 + z];
+        cplx<T> &c = bufA[prow<FM2>(p, mk2) + z];
         const int r0 = 2 * p * m2 + z;
         const T e0 = E4s[r0];
         c.x *= e0 * e0;
@@ -461,7 +472,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
         mbar_wait(&bars[2], 0, a.err);
         for (int e = threadIdx.x; e < npz; e += MT) {
             const int p = e / m2, z = e - p * m2;
-            const cplx<T> c = buf[2 * p * mk2 + z];
+            const cplx<T> c = buf[prow<FM2>(p, mk2) + z];
             const int r0 = 2 * p * m2 + z;
             // Richardson, GPU_kernels.h:199-203
             const T q0 = (c.x * E[r0] * (T)4 - Q[r0]) / (T)3;
@@ -491,7 +502,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
         const int p = e / m2, z = e - p * m2;
         const int r0 = 2 * p * m2 + z;
         const bool hb = 2 * p + 1 < m1;
-        buf[2 * p * mk2 + z] = {Q[r0] * En[r0], hb ? Q[r0 + m2] * En[r0 + m2] : (T)0};
+        buf[prow<FM2>(p, mk2) + z] = {Q[r0] * En[r0], hb ? Q[r0 + m2] * En[r0 + m2] : (T)0};
     }
     __syncthreads();
     slab_forward_fixed<T, m1, m2, MT>(buf, twy, twz);
@@ -507,7 +518,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
             const T e1 = En[r0 + m2];
             v1 = Q[r0 + m2] * (e1 * e1);
         }
-        buf[2 * p * mk2 + z] = {Q[r0] * (e0 * e0), v1};
+        buf[prow<FM2>(p, mk2) + z] = {Q[r0] * (e0 * e0), v1};
     }
     __syncthreads();
     slab_forward_fixed<T, m1, m2, MT>(buf, twy, twz);

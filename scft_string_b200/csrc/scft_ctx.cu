@@ -1422,26 +1422,34 @@ scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, 
 
 // Variable-cell relaxation of replica ii: `inner` SCFT iterations (the
 // solve_field loop restricted to this replica, scft.cu:598-608, without the
-// periodic FreeE), then L_i -= gamma dF/dL_i with each relative change capped
-// at 2 %, until max |dF/dL_i| <= stressTol.
+// periodic FreeE) or, with inner <= 0, an Anderson re-solve to RMS 1e-9; then
+// L_i -= gamma dF/dL_i with each relative change capped at 2 %, until
+// max |dF/dL_i| <= stressTol.
 scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, double stressTol, double gamma,
                             int *outer_out, double *stress_out)
 {
-    if (!ctx || ii < 0 || ii >= ctx->strn || inner < 1 || maxOuter < 1 || !(gamma > 0)) return SCFT_BAD_INPUT;
+    if (!ctx || ii < 0 || ii >= ctx->strn || maxOuter < 1 || !(gamma > 0)) return SCFT_BAD_INPUT;
     double dF[3] = {0, 0, 0};
     int outer = 0;
     scft_status s = SCFT_OK;
     for (; outer < maxOuter; outer++) {
-        s = scft_string_begin(ctx, ii, inner, 1e-3);
-        if (s != SCFT_OK) return s;
-        ctx->sf.skip_freee = true;
-        for (int k = 0; k < inner; k++) {
-            int done = 0;
-            s = scft_string_step(ctx, nullptr, nullptr, nullptr, &done);
+        if (inner <= 0) {  // Anderson re-solve of the fields at the current box
+            int it = 0;
+            double e = 0;
+            s = scft_anderson_solve(ctx, ii, 3000, 1e-9, 12, 0.1, &it, &e);
             if (s != SCFT_OK) return s;
-            if (done) break;
+        } else {
+            s = scft_string_begin(ctx, ii, inner, 1e-3);
+            if (s != SCFT_OK) return s;
+            ctx->sf.skip_freee = true;
+            for (int k = 0; k < inner; k++) {
+                int done = 0;
+                s = scft_string_step(ctx, nullptr, nullptr, nullptr, &done);
+                if (s != SCFT_OK) return s;
+                if (done) break;
+            }
+            scft_string_end(ctx, nullptr);
         }
-        scft_string_end(ctx, nullptr);
         s = scft_stress(ctx, ii, nullptr, dF);
         if (s != SCFT_OK) return s;
         const double mx = std::max(std::fabs(dF[0]), std::max(std::fabs(dF[1]), std::fabs(dF[2])));
@@ -1506,6 +1514,54 @@ scft_status scft_reset_stats(scft_ctx *ctx)
 {
     if (!ctx) return SCFT_BAD_INPUT;
     ctx->stats = scft_stats{};
+    return SCFT_OK;
+}
+
+// Times props rounds of every replica with one and with two concurrent slot
+// groups (each candidate re-captures its graphs, one untimed round, then the
+// fastest of three timed rounds) and keeps the faster setting.  The rounds
+// recompute every replica's densities at its current fields, so the state a
+// caller sees afterwards is unchanged; the statistics are restored.
+scft_status scft_autotune(scft_ctx *ctx, int *groups_out, double *times_ms)
+{
+    if (!ctx) return SCFT_BAD_INPUT;
+    const scft_stats keep = ctx->stats;
+    std::vector<int> all(ctx->strn);
+    for (int i = 0; i < ctx->strn; i++) all[i] = i;
+    double best = 0;
+    int best_g = 1;
+    for (int ng = 1; ng <= 2; ng++) {
+        for (auto &g : ctx->graphs)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        ctx->ngroups = ng;
+        scft_status s = props_list(ctx, all);
+        if (s != SCFT_OK) return s;
+        double t = 1e300;
+        for (int r = 0; r < 3; r++) {
+            const double before = ctx->stats.props_seconds;
+            s = props_list(ctx, all);
+            if (s != SCFT_OK) return s;
+            t = std::min(t, (ctx->stats.props_seconds - before) * 1e3);
+        }
+        if (times_ms) times_ms[ng - 1] = t;
+        if (ng == 1 || t < best) {
+            best = t;
+            best_g = ng;
+        }
+    }
+    if (best_g != ctx->ngroups) {
+        for (auto &g : ctx->graphs)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        ctx->ngroups = best_g;
+    }
+    ctx->stats = keep;
+    if (groups_out) *groups_out = best_g;
     return SCFT_OK;
 }
 

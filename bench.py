@@ -282,8 +282,9 @@ def run_mixed128(a):
 def run_adjoint96(a):
     """64x64x96, N=160 single replica: converged saddle point (Anderson), box
     stress from the FP64 and FP32 adjoints against central differences of
-    re-converged FP64 free energies (h = 1e-4), dF/dchiN likewise, then
-    variable-cell relaxation to |stress| <= 1e-6."""
+    re-converged FP64 free energies (h = 1e-4), dF/dchiN likewise, dF/df with a
+    continuous A fraction against one-sided differences, then variable-cell
+    relaxation to |stress| <= 1e-6."""
     import numpy as np
     import torch
 
@@ -294,8 +295,10 @@ def run_adjoint96(a):
     wm, wp = hex_fields(c)
     t0 = time.time()
 
-    def converged(D, chi, prec="fp64", W0=None):
+    def converged(D, chi, prec="fp64", W0=None, f=None):
         cc = dict(c, D=tuple(D), chi=chi)
+        if f is not None:  # continuous A fraction
+            cc.update(f=f, fcont=1)
         ctx = S.StringSolver(cc, precision=prec)
         if W0 is None:
             ctx.set_fields(0, wm[0], wp[0])
@@ -309,10 +312,12 @@ def run_adjoint96(a):
     ctx, F0, err0, n0 = converged(D0, c["chi"])
     W = ctx.get_fields(0)
     _, dF64 = ctx.stress(0)
+    _, dF64ck, bytes64 = ctx.stress_ckpt(0, 13)   # q kept every 13 contour steps
     c32 = S.StringSolver(c, precision="fp32")
     c32.set_fields_2m(0, np.ascontiguousarray(W))
-    _, dF32 = c32.stress(0)
+    _, dF32, bytes32 = c32.stress_ckpt(0, 13)
     c32.close()
+    store32 = (c["N"] + 1) * 2 * ctx.M * 4
     h = 1e-4
     fd = []
     for i in range(3):
@@ -329,6 +334,22 @@ def run_adjoint96(a):
     cm, Fcm, _, _ = converged(D0, c["chi"] - h, W0=W)
     cm.close()
     fdc = (Fcp - Fcm) / (2 * h)
+    # dF/df with a continuous A fraction: N f = 64 lies on a step boundary, so the
+    # adjoint gives the right derivative; second-order one-sided differences
+    f0 = c["f"]
+    cf0, Ff0, _, _ = converged(D0, c["chi"], W0=W, f=f0)
+    dFdf = cf0.dF_df(0)[1]
+    cf32 = S.StringSolver(dict(c, fcont=1), precision="fp32")
+    cf32.set_fields_2m(0, np.ascontiguousarray(cf0.get_fields(0)))
+    dFdf32 = cf32.dF_df(0)[1]
+    cf32.close()
+    cf0.close()
+    Ff = [Ff0]
+    for k in (1, 2):
+        ck_, Fk, _, _ = converged(D0, c["chi"], W0=W, f=f0 + k * h)
+        ck_.close()
+        Ff.append(Fk)
+    fdf = (-3 * Ff[0] + 4 * Ff[1] - Ff[2]) / (2 * h)
     relax = None
     if err0 < 1e-7:  # relax from a converged saddle only
         n, st, box = ctx.relax_cell(0, maxOuter=20, inner=0, stressTol=1e-6, gamma=2.0)
@@ -336,9 +357,13 @@ def run_adjoint96(a):
     out = {"workload": c["name"], "saddle_residual": err0, "anderson_iters": n0, "F": F0,
            "dF_dL_fp64_adjoint": list(dF64), "dF_dL_fp32_adjoint": list(dF32), "dF_dL_fd": fd,
            "dF_dL_fp32_vs_fp64_rel": float(np.max(np.abs(dF32 - dF64)) / max(1e-30, np.max(np.abs(dF64)))),
+           "dF_dL_fp64_ckpt13_vs_full": float(np.max(np.abs(dF64ck - dF64))),
+           "ckpt13_bytes_fp32": bytes32, "full_store_bytes_fp32": store32,
            "dF_dchi_closed_form": dchi, "dF_dchi_fd": fdc,
+           "dF_df_fp64_adjoint": dFdf, "dF_df_fp32_adjoint": dFdf32, "dF_df_fd_one_sided": fdf,
            "relax": relax,
-           "checkpointing": "all q slices stored (no sqrt(N) recompute)", "wall_s": time.time() - t0}
+           "checkpointing": "FP32 adjoint with q, q^dagger kept every 13 contour steps (scft_stress_ckpt)",
+           "wall_s": time.time() - t0}
     print(json.dumps(out))
     return 0
 

@@ -47,7 +47,8 @@ typedef struct {
     int    ens;         /* 1 canonical, 2 grand canonical */
     double phidb;       /* copolymer volume fraction (ens 1) or fugacity (ens 2) */
     double chi;         /* chi*N */
-    double f;           /* A fraction of the copolymer; rounded to round(N f)/N as scft.cu:1008 */
+    double f;           /* A fraction of the copolymer; rounded to round(N f)/N as scft.cu:1008
+                         * unless fcont */
     int    strn;        /* replicas on the string, 1..64 */
     int    fix[2];      /* keep the first / last replica fixed */
     int    dostring;    /* 1: string method, 0: independent replicas */
@@ -55,6 +56,10 @@ typedef struct {
     int    precision;   /* scft_precision of the propagator bulk (reductions are FP64) */
     int    batched;     /* 1: all replicas advance together; 0: one replica at a time */
     int    device;      /* CUDA device ordinal */
+    int    fcont;       /* 0: the reference's rounded f.  1: continuous A fraction (no
+                         * reference counterpart): n1 = floor(N f) whole A steps, and step
+                         * n1 sees the field theta wA + (1-theta) wB, theta = N f - n1, with
+                         * theta of its Simpson weight moved from B to A; needs Nh < N - n1 */
 } scft_problem;
 
 typedef struct scft_ctx scft_ctx;
@@ -148,6 +153,18 @@ scft_status scft_get_box(const scft_ctx *ctx, double *D);
  * stress dF/dL_i = -d lnQ/dL_i, exact at a converged saddle point.  Either
  * output may be NULL. */
 scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL);
+/* The same derivatives with the propagators held only at checkpoints at most
+ * K contour steps apart (K ~ sqrt(N)): one forward pass keeps the checkpoint
+ * slices, then every segment is recomputed once next to its mirror segment
+ * (two chain passes in all).  Device memory: *bytes_out (may be NULL) instead
+ * of the (N+1) slice pairs of the full store; the context's full store is not
+ * touched.  Same values as scft_stress up to the order of the FP64 sums. */
+/* d lnQ/df and dF/df = -d lnQ/df (exact at a converged saddle point) of
+ * replica ii, for a context created with fcont = 1: the adjoint of the
+ * junction step, whose field depends on f.  Either output may be NULL. */
+scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df);
+scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL,
+                             double *bytes_out);
 /* Anderson-accelerated solution of replica ii's field equations (an option
  * beside the reference's simple mixing; no reference counterpart): residual
  * as scft.cu:605-607 without spring or string terms, history of nhist

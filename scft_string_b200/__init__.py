@@ -52,6 +52,7 @@ class Problem(C.Structure):
         ("precision", C.c_int),
         ("batched", C.c_int),
         ("device", C.c_int),
+        ("fcont", C.c_int),
     ]
 
 
@@ -75,7 +76,7 @@ EXPORTS = [
     "scft_free_energy", "scft_last_free_energy", "scft_spline_derivs", "scft_spline_redist", "scft_get_stats",
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
-    "scft_anderson_solve", "scft_autotune",
+    "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
 ]
 
 _lib = None
@@ -132,6 +133,8 @@ def lib():
     L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
     L.scft_autotune.argtypes = [vp, _ip, _dp]
+    L.scft_stress_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
+    L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
     _lib = L
     return L
 
@@ -152,7 +155,7 @@ class Context:
     """An scft_ctx: every replica of one problem resident on one B200."""
 
     def __init__(self, m, D, N, chi, f, phidb, ens=2, alpha=0.1, strn=1, fix=(0, 0),
-                 dostring=1, springsteps=0, precision="fp64", batched=True, device=0):
+                 dostring=1, springsteps=0, precision="fp64", batched=True, device=0, fcont=0):
         p = Problem()
         p.m = (C.c_int * 3)(*[int(v) for v in m])
         p.D = (C.c_double * 3)(*[float(v) for v in D])
@@ -163,6 +166,7 @@ class Context:
         p.precision = SCFT_FP32 if str(precision).lower() in ("fp32", "float32", "1") else SCFT_FP64
         p.batched = 1 if batched else 0
         p.device = int(device)
+        p.fcont = int(fcont)
         self.problem = p
         self.m = tuple(int(v) for v in m)
         self.M = int(np.prod(self.m))
@@ -332,6 +336,13 @@ class Context:
         self._ck(lib().scft_stress(self.h, int(ii), _p(a), _p(b)))
         return a, b
 
+    def stress_ckpt(self, ii=0, K=13):
+        """(d lnQ/dL, dF/dL, device bytes) by the adjoint with checkpoints K steps apart."""
+        a, b = np.zeros(3), np.zeros(3)
+        nb = C.c_double()
+        self._ck(lib().scft_stress_ckpt(self.h, int(ii), int(K), _p(a), _p(b), C.byref(nb)))
+        return a, b, nb.value
+
     def anderson_solve(self, ii=0, maxIter=2000, tol=1e-10, nhist=10, lam=0.1):
         """Anderson-mixing solve of replica ii; returns (iterations, RMS residual)."""
         n = C.c_int()
@@ -347,6 +358,12 @@ class Context:
         self._ck(lib().scft_relax_cell(self.h, int(ii), int(maxOuter), int(inner), float(stressTol),
                                        float(gamma), C.byref(n), _p(st)))
         return n.value, st, self.get_box()
+
+    def dF_df(self, ii=0):
+        """(d lnQ/df, dF/df) of replica ii; the context needs fcont=1."""
+        a, b = C.c_double(), C.c_double()
+        self._ck(lib().scft_dF_df(self.h, int(ii), C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def dF_dchi(self, ii=0):
         v = C.c_double()
@@ -388,4 +405,5 @@ def StringSolver(cfg: dict, precision="fp64", batched=True, springsteps=0, devic
     return Context(cfg["m"], cfg["D"], cfg["N"], chi=cfg["chi"], f=cfg["f"], phidb=cfg["phidb"],
                    ens=cfg["ens"], alpha=cfg.get("alpha", 0.1), strn=cfg["strn"],
                    fix=cfg.get("fix", (0, 0)), dostring=cfg.get("dostring", 1),
-                   springsteps=springsteps, precision=precision, batched=batched, device=device)
+                   springsteps=springsteps, precision=precision, batched=batched, device=device,
+                   fcont=cfg.get("fcont", 0))

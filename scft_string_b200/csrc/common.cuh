@@ -56,6 +56,10 @@ struct Geo {
     int Ns, n1, n2, Nh;
     int ncol_tiles;  // x-pencil tiles per field
     int tc;          // columns per x-pencil tile
+    // continuous A fraction (off when jon == 0): q's step jq and q^dagger's
+    // step jqd see the junction field theta wA + (1 - theta) wB (E table 2)
+    int jon, jq, jqd;
+    double theta;
 };
 
 }  // namespace scft

@@ -41,6 +41,7 @@ struct PropsArgs {
     int ens;
     int *err;               // device error word (launch-geometry / plan errors)
     int slot0;              // first slot of this launch within the spectra tensor map
+    T *jtab;                // [slot][M]  junction-step E4 (continuous A fraction only)
 };
 
 struct PropsLaunch {
@@ -68,6 +69,15 @@ template <typename T>
 int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st);
 template <typename T>
 int set_props_smem(const PropsLaunch &L);
+// chain segment of slot 0 (a.g.Ns steps; a.g.n1, n2 relative to the segment
+// start), E tables of slot 0 from its replica, Q2/QC/lnQ of slot 0 from the
+// store slices a.g.Ns (q) and a.g.Nh (q^dagger)
+template <typename T>
+int launch_chain(const PropsArgs<T> &a, const PropsLaunch &L, int first_mode, cudaStream_t st);
+template <typename T>
+int launch_prepare(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st);
+template <typename T>
+int launch_qsums(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st);
 
 // ------------------------------------------------------------------ stress (adjoint)
 constexpr int kStressPairs = 16;
@@ -91,6 +101,9 @@ struct StressArgs {
     double L[3];
     T invM;
     int *err;
+    const T *jtab;           // [slot][M] junction-step E4 (table 2), continuous A fraction only
+    T *rbuf;                 // [6][M] real work arrays of the junction derivative
+    const double *wminus;    // W- of the replica (junction derivative)
 };
 
 template <typename T>
@@ -98,6 +111,12 @@ int launch_stress_chunk(const StressArgs<T> &a, const StressPairs &P, int slab_t
                         int pencil_threads, int pencil_smem, double *out, cudaStream_t st);
 template <typename T>
 int set_stress_smem(int slab_smem, int pencil_smem);
+// <y, dS_J/dtheta x> of the junction step (pair 0 of P, table 2) summed over
+// the grid: block partials into `part` (nblk), then `out` (one double)
+template <typename T>
+int launch_junction_dtheta(const StressArgs<T> &a, const StressPairs &P, int slab_threads, int slab_smem,
+                           int pencil_threads, int pencil_smem, double *part, int nblk, double *out,
+                           cudaStream_t st);
 
 // ------------------------------------------------------------------ FP64 field kernels
 constexpr int kMaxStrn = 64;

@@ -37,6 +37,7 @@ constexpr size_t kNoAllocDoubles = 16 * (size_t)kNoAllocMaxM + 9 * kNoAllocMaxAx
 constexpr size_t kNoAllocBytes = kNoAllocDoubles * sizeof(double);
 
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+static_assert(sizeof(g_noalloc_scratch) == kNoAllocBytes, "scratch size");
 
 // device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
 void *g_scratch_addr[kNoAllocMaxDevices];

@@ -28,11 +28,21 @@ __device__ __forceinline__ size_t hist_off(const Geo &g, int slot, int s, int fl
     return (((size_t)slot * (g.Ns + 1) + s) * 2 + fld) * (size_t)g.M;
 }
 
-// E4 table (0: A field, 1: B field) for field fld (0: q, 1: q^dagger) at step s;
-// q sees the A block for s < n1, q^dagger the B block for s < n2 (density.h:136-146)
+// E4 table (0: A field, 1: B field, 2: junction) for field fld (0: q,
+// 1: q^dagger) at step s; q sees the A block for s < n1, q^dagger the B block
+// for s < n2 (density.h:136-146).  With a continuous A fraction the step that
+// holds the junction (q's jq, q^dagger's jqd) takes table 2.
 __device__ __forceinline__ int etab_sel(const Geo &g, int fld, int s)
 {
+    if (g.jon && s == (fld == 0 ? g.jq : g.jqd)) return 2;
     return fld == 0 ? (s < g.n1 ? 0 : 1) : (s < g.n2 ? 1 : 0);
+}
+
+// the E4 table `sel` of slot `slot`
+template <typename T>
+__device__ __forceinline__ const T *etab_ptr(const PropsArgs<T> &a, int slot, int sel)
+{
+    return sel == 2 ? a.jtab + (size_t)slot * a.g.M : a.etab + ((size_t)slot * 2 + sel) * a.g.M;
 }
 
 template <typename T>
@@ -57,6 +67,8 @@ __global__ void k_prepare(PropsArgs<T> a)
         const double wm = W[r], wp = W[r + g.M];
         e[r] = (T)exp(-(wm + wp) * ds / 4);
         e[r + g.M] = (T)exp(-(-wm + wp) * ds / 4);
+        // junction step: theta wA + (1 - theta) wB = W+ + (2 theta - 1) W-
+        if (g.jon) a.jtab[(size_t)slot * g.M + r] = (T)exp(-(wp + (2.0 * g.theta - 1.0) * wm) * ds / 4);
     }
 }
 
@@ -122,7 +134,6 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2;  // real offset of this slab
     const size_t slab_k = (size_t)x * m1 * mk2;
-    const T *etab = a.etab + (size_t)slot * 2 * M;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     cplx<T> *specB = specA + Mk;
     const int sn = s + 1;
@@ -133,7 +144,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
         for (int i = threadIdx.x; i < m1 * mk2; i += nthr) buf[i] = specA[slab_k + i];
         __syncthreads();
         slab_inv<T, MT, FM1, FM2>(buf, g, twy, twz, a.err);
-        const T *E4 = etab + (size_t)etab_sel(g, fld, s) * M + slab_r;
+        const T *E4 = etab_ptr(a, slot, etab_sel(g, fld, s)) + slab_r;
         const T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
         for (int e = threadIdx.x; e < npz; e += nthr) {
             const int p = e / m2, z = e - p * m2;
@@ -169,7 +180,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     }
     if (sn >= g.Ns) return;
     __syncthreads();
-    const T *E4n = etab + (size_t)etab_sel(g, fld, sn) * M + slab_r;
+    const T *E4n = etab_ptr(a, slot, etab_sel(g, fld, sn)) + slab_r;
     // half step input E4' q'
     for (int e = threadIdx.x; e < npz; e += nthr) {
         const int p = e / m2, z = e - p * m2;
@@ -218,7 +229,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2;
     const size_t slab_k = (size_t)x * m1 * mk2;
-    const T *E4 = a.etab + (size_t)slot * 2 * M + (size_t)etab_sel(g, fld, s) * M + slab_r;
+    const T *E4 = etab_ptr(a, slot, etab_sel(g, fld, s)) + slab_r;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     cplx<T> *specB = specA + Mk;
     T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
@@ -363,7 +374,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     T *E4s = reinterpret_cast<T *>(twz + m2);
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
-    const T *E4g = a.etab + (size_t)slot * 2 * M + (size_t)etab_sel(g, fld, s) * M + slab_r;
+    const T *E4g = etab_ptr(a, slot, etab_sel(g, fld, s)) + slab_r;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     cplx<T> *specB = specA + Mk;
     T *P = a.pbuf + ((size_t)slot * 2 + fld) * M + slab_r;
@@ -433,7 +444,6 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     T *E = Q + L::REAL;                        // E4 of step s (or of step s+1)
     const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
-    const T *etab = a.etab + (size_t)slot * 2 * M;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     cplx<T> *specB = specA + Mk;
     const int sn = s + 1;
@@ -444,7 +454,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     // E holds the table of step s; the next step reads it from shared memory
     // unless it switches blocks there (s+1 == n1 or n2), then from global
     const bool e_next_shared = sel_s == sel_n;
-    const T *E4n_g = etab + (size_t)sel_n * M + slab_r;
+    const T *E4n_g = etab_ptr(a, slot, sel_n) + slab_r;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 3; i++) mbar_init(&bars[i], 1);
         mbar_fence_init();
@@ -459,7 +469,7 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
         }
         if (mode == 0 || next) {
             mbar_expect_tx(&bars[2], L::REAL_BYTES);
-            bulk_g2s(E, etab + (size_t)sel_s * M + slab_r, L::REAL_BYTES, &bars[2]);
+            bulk_g2s(E, etab_ptr(a, slot, sel_s) + slab_r, L::REAL_BYTES, &bars[2]);
         }
     }
     for (int i = threadIdx.x; i < m1; i += MT) twy[i] = a.tw[FM0 + i];
@@ -704,6 +714,14 @@ __global__ void k_density(PropsArgs<T> a)
         for (s = 1, wt = 4; s < Nh; s++, wt = 6 - wt) kahan_add(rhB, chB, wt * Q2(s) * Q2(Nh - s));
         for (s = 1, wt = 4; s < n1; s++, wt = 6 - wt) kahan_add(rCA, cA, wt * Q1(s) * Q2(Ns - s));
         for (s = n1 + 1, wt = 4; s < Ns; s++, wt = 6 - wt) kahan_add(rCB, cB, wt * Q1(s) * Q2(Ns - s));
+        if (g.jon) {
+            // continuous A fraction: theta of the junction step's trapezoid
+            // weight moves from the B block to the A block (3/2 here: the sums
+            // are scaled by ds/3 below)
+            const double tj = 1.5 * g.theta * (Q1(n1) * Q2(Ns - n1) + Q1(n1 + 1) * Q2(Ns - n1 - 1));
+            rCA += tj;
+            rCB -= tj;
+        }
 #undef Q1
 #undef Q2
         const double rhA = 0.0;  // the A-homopolymer density is scaled by zA = 0
@@ -825,6 +843,25 @@ int launch_single_step_mt(const PropsArgs<T> &a, const PropsLaunch &L, int s, cu
     return 6;
 }
 
+// A chain segment of slot 0 (checkpointed adjoint): q and q^dagger advanced
+// g.Ns steps from store slice 0 (first_mode 2) or from q = 1 (first_mode 1).
+// The segment's Geo carries n1 and n2 minus the segment's first contour index,
+// so every step picks the E table of its absolute index.
+template <typename T, int MT, int F0, int F1, int F2>
+int launch_chain_mt(const PropsArgs<T> &a, const PropsLaunch &L, int first_mode, cudaStream_t st)
+{
+    const Geo &g = a.g;
+    dim3 gs(g.m0, 2, 1), gp(g.ncol_tiles, 2, 1);
+    launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, first_mode, st);
+    for (int s = 0; s < g.Ns; s++) {
+        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 1, st);
+        launch_mid<T, MT, F0, F1, F2>(a, L, gs, s, st);
+        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 0, st);
+        launch_combine<T, MT, F0, F1, F2>(a, L, gs, s, 0, st);
+    }
+    return 1 + 4 * g.Ns;
+}
+
 template <typename T, int MT, int F0, int F1, int F2>
 int set_smem_mt(const PropsLaunch &L)
 {
@@ -866,12 +903,13 @@ void pf_smem_bytes(int id, int fp32, int &mid, int &comb)
         pf_smem<double>(id, mid, comb);
 }
 
-// op 0: props, 1: single step, 2: shared-memory attributes
+// op 0: props, 1: single step, 2: shared-memory attributes, 3: chain segment
 template <typename T, int MT, int F0, int F1, int F2>
 int run_op(int op, const PropsArgs<T> *a, const PropsLaunch &L, int n, cudaStream_t st)
 {
     if (op == 0) return launch_props_mt<T, MT, F0, F1, F2>(*a, L, n, st);
     if (op == 1) return launch_single_step_mt<T, MT, F0, F1, F2>(*a, L, n, st);
+    if (op == 3) return launch_chain_mt<T, MT, F0, F1, F2>(*a, L, n, st);
     return set_smem_mt<T, MT, F0, F1, F2>(L);
 }
 
@@ -918,11 +956,38 @@ int set_props_smem(const PropsLaunch &L)
     return dispatch<T>(2, nullptr, L, 0, nullptr);
 }
 
+template <typename T>
+int launch_chain(const PropsArgs<T> &a, const PropsLaunch &L, int first_mode, cudaStream_t st)
+{
+    return dispatch<T>(3, &a, L, first_mode, st);
+}
+
+template <typename T>
+int launch_prepare(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st)
+{
+    k_prepare<T><<<dim3(L.ew_blocks, 1), 256, 0, st>>>(a);
+    return 1;
+}
+
+template <typename T>
+int launch_qsums(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st)
+{
+    k_qsum<T><<<dim3(L.red_blocks, 1), 256, 0, st>>>(a);
+    k_qfinal<T><<<1, 32, 0, st>>>(a, L.red_blocks);
+    return 2;
+}
+
 template int launch_props<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);
 template int launch_props<double>(const PropsArgs<double> &, const PropsLaunch &, int, cudaStream_t);
 template int launch_single_step<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);
 template int launch_single_step<double>(const PropsArgs<double> &, const PropsLaunch &, int, cudaStream_t);
 template int set_props_smem<float>(const PropsLaunch &);
 template int set_props_smem<double>(const PropsLaunch &);
+template int launch_chain<float>(const PropsArgs<float> &, const PropsLaunch &, int, cudaStream_t);
+template int launch_chain<double>(const PropsArgs<double> &, const PropsLaunch &, int, cudaStream_t);
+template int launch_prepare<float>(const PropsArgs<float> &, const PropsLaunch &, cudaStream_t);
+template int launch_prepare<double>(const PropsArgs<double> &, const PropsLaunch &, cudaStream_t);
+template int launch_qsums<float>(const PropsArgs<float> &, const PropsLaunch &, cudaStream_t);
+template int launch_qsums<double>(const PropsArgs<double> &, const PropsLaunch &, cudaStream_t);
 
 }  // namespace scft

@@ -77,6 +77,7 @@ struct scft_ctx {
     double *partials = nullptr, *redout = nullptr;
     int npart_stride = 0, nred_rows = 0;
     int *rep_dev = nullptr, *err = nullptr;
+    void *jtab = nullptr;  // junction-step E table per slot (continuous A fraction)
     void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
          *kfac = nullptr;
     SplineKnots *knots = nullptr;
@@ -86,6 +87,9 @@ struct scft_ctx {
     double *and_X = nullptr, *and_D = nullptr;  // Anderson histories
     int and_H = 0;
     double *st_part = nullptr, *st_out = nullptr;
+    void *jd_rbuf = nullptr;  // junction derivative: six real work arrays
+    void *ck_mem = nullptr;  // checkpointed adjoint: checkpoints, two segments, Q slices
+    size_t ck_bytes = 0;
     int rt_slab_threads = 0, rt_slab_smem = 0, rt_pencil_threads = 0, rt_pencil_smem = 0;
 
     // one captured CUDA graph per (chunk offset, batch size) of a props round
@@ -151,6 +155,7 @@ PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
     a.ens = ctx->p.ens;
     a.err = ctx->err;
     a.slot0 = 0;
+    a.jtab = (T *)ctx->jtab;
     return a;
 }
 
@@ -167,6 +172,7 @@ PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0)
     a.pbuf += (size_t)s0 * 2 * M;
     a.partials += (size_t)s0 * ctx->npart_stride;
     a.slot0 = s0;
+    if (a.jtab) a.jtab += (size_t)s0 * M;
     return a;
 }
 
@@ -530,7 +536,7 @@ void scft_destroy(scft_ctx *ctx)
     void *ptrs[] = {ctx->W, ctx->conc, ctx->DEV, ctx->dWda, ctx->rs, ctx->partials, ctx->redout,
                     ctx->rep_dev, ctx->err, ctx->etab, ctx->hist, ctx->spec, ctx->pbuf, ctx->tw,
                     ctx->kfac, ctx->knots, ctx->st_S4, ctx->st_S2, ctx->st_S4p, ctx->st_part,
-                    ctx->st_out, ctx->and_X, ctx->and_D};
+                    ctx->st_out, ctx->and_X, ctx->and_D, ctx->ck_mem, ctx->jtab, ctx->jd_rbuf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : ctx->tev)
@@ -565,12 +571,25 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
     g.Mk = g.m0 * g.m1 * g.mk2;
     g.npair = (g.m1 + 1) / 2;
     g.slab_c = g.m1 * g.mk2 + g.m2 + 32;
-    const double f = std::round(p->N * p->f) / p->N;  // scft.cu:1008
+    if (!(p->f >= 0 && p->f <= 1) || p->N < 1) return SCFT_BAD_INPUT;
+    const double f = p->fcont ? p->f : std::round(p->N * p->f) / p->N;  // scft.cu:1008
     g.Ns = p->N;
-    g.n1 = (int)std::round(g.Ns * f);  // density.h:346
+    g.n1 = p->fcont ? (int)std::floor(g.Ns * f) : (int)std::round(g.Ns * f);  // density.h:346
     g.n2 = g.Ns - g.n1;
     g.Nh = (int)(p->alpha * g.Ns);
+    g.jon = 0;
+    g.jq = g.jqd = -1;
+    g.theta = 0;
     if (g.n1 < 0 || g.n1 > g.Ns || g.Nh > g.Ns) return SCFT_BAD_INPUT;
+    if (p->fcont) {
+        // junction inside q's step n1 = q^dagger's step N-1-n1; the homopolymer
+        // (q^dagger's first Nh steps) must stay in the pure B block
+        if (g.n1 >= g.Ns || g.Nh > g.n2 - 1) return SCFT_BAD_INPUT;
+        g.jon = 1;
+        g.jq = g.n1;
+        g.jqd = g.n2 - 1;
+        g.theta = g.Ns * f - g.n1;
+    }
 
     int dev = p->device;
     cudaDeviceProp prop;
@@ -665,6 +684,7 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMalloc(&ctx->rep_dev, sizeof(int) * (R + 1)));
         CKC(cudaMalloc(&ctx->err, sizeof(int)));
         CKC(cudaMalloc(&ctx->etab, T * 2 * M * S));
+        if (g.jon) CKC(cudaMalloc(&ctx->jtab, T * M * S));
         CKC(cudaMalloc(&ctx->hist, T * 2 * M * (size_t)(g.Ns + 1) * S));
         CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
         CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
@@ -795,8 +815,8 @@ scft_status scft_props_host(scft_ctx *ctx, double *w, double *lnQ, int ii, int N
 {
     (void)ii;
     if (!ctx || !w) return SCFT_BAD_INPUT;
-    if (Ns != ctx->g.Ns || alpha != ctx->p.alpha || phic != ctx->p.phidb ||
-        (int)std::round(Ns * f) != ctx->g.n1) {
+    const bool f_ok = ctx->g.jon ? std::fabs(f - ctx->f) <= 1e-12 : (int)std::round(Ns * f) == ctx->g.n1;
+    if (Ns != ctx->g.Ns || alpha != ctx->p.alpha || phic != ctx->p.phidb || !f_ok) {
         ctx->lasterr = "scft_props_host: Ns/alpha/phic/f differ from the context";
         return SCFT_BAD_INPUT;
     }
@@ -1234,42 +1254,47 @@ scft_status scft_get_box(const scft_ctx *ctx, double *D)
 // d lnQ / d L_i of replica ii at its current fields, by the adjoint of the
 // propagator (stress_kernels.cu); the free energy's box derivative at the
 // saddle point is dF/dL = -dlnQ/dL (the field terms carry no explicit L).
-scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
+}  // extern "C"
+
+namespace {
+
+// one adjoint pair <y, dS/dL x>: slices (xs, xf) and (ys, yf) of the store at
+// `hist` (slot `slot`), E table `sel`, homopolymer (Q2) or copolymer (QC) sum
+struct StressPr {
+    int xs, xf, ys, yf, sel, homo;
+};
+
+scft_status stress_alloc(scft_ctx *ctx)
 {
-    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    if (ctx->st_S4) return SCFT_OK;
     const Geo &g = ctx->g;
     const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
-    if (!ctx->st_S4) {
-        const size_t sz = T * 2 * 2 * (size_t)g.Mk * kStressPairs;
-        CK(cudaMalloc(&ctx->st_S4, sz));
-        CK(cudaMalloc(&ctx->st_S2, sz));
-        CK(cudaMalloc(&ctx->st_S4p, sz));
-        CK(cudaMalloc(&ctx->st_part, sizeof(double) * 9 * (size_t)g.ncol_tiles * kStressPairs));
-        CK(cudaMalloc(&ctx->st_out, sizeof(double) * 3 * kStressPairs));
-        if ((T == 4 ? set_stress_smem<float>(ctx->rt_slab_smem, ctx->rt_pencil_smem)
-                    : set_stress_smem<double>(ctx->rt_slab_smem, ctx->rt_pencil_smem)) != 0) {
-            ctx->lasterr = "stress kernels: shared memory attribute";
-            return SCFT_CUDA_ERROR;
-        }
+    const size_t sz = T * 2 * 2 * (size_t)g.Mk * kStressPairs;
+    CK(cudaMalloc(&ctx->st_S4, sz));
+    CK(cudaMalloc(&ctx->st_S2, sz));
+    CK(cudaMalloc(&ctx->st_S4p, sz));
+    CK(cudaMalloc(&ctx->st_part, sizeof(double) * 9 * (size_t)g.ncol_tiles * kStressPairs));
+    CK(cudaMalloc(&ctx->st_out, sizeof(double) * 3 * kStressPairs));
+    if ((T == 4 ? set_stress_smem<float>(ctx->rt_slab_smem, ctx->rt_pencil_smem)
+                : set_stress_smem<double>(ctx->rt_slab_smem, ctx->rt_pencil_smem)) != 0) {
+        ctx->lasterr = "stress kernels: shared memory attribute";
+        return SCFT_CUDA_ERROR;
     }
-    // fresh propagators of replica ii
-    scft_status s = props_list(ctx, {ii});
-    if (s != SCFT_OK) return s;
-    const int slot = ctx->slot_of[ii];
-    const double Q2 = rsv(ctx, ii, kRsQ2), QC = rsv(ctx, ii, kRsQC);
-    // pairs: copolymer (q(s), q^dagger(N-1-s)), homopolymer (q^dagger(j), q^dagger(Nh-1-j))
-    struct Pr { int xs, xf, ys, yf, sel, homo; };
-    std::vector<Pr> pairs;
-    for (int s2 = 0; s2 < g.Ns; s2++) pairs.push_back({s2, 0, g.Ns - 1 - s2, 1, s2 < g.n1 ? 0 : 1, 0});
-    for (int j = 0; j < g.Nh; j++) pairs.push_back({j, 1, g.Nh - 1 - j, 1, 1, 1});
-    double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
+    return SCFT_OK;
+}
+
+// sums the pairs (in chunks of kStressPairs) into dQC / dQ2 (unnormalised)
+scft_status stress_pairs(scft_ctx *ctx, int slot, const void *hist, const std::vector<StressPr> &pairs,
+                         double *dQC, double *dQ2)
+{
+    const Geo &g = ctx->g;
     std::vector<double> out(3 * kStressPairs);
     for (size_t c0 = 0; c0 < pairs.size(); c0 += kStressPairs) {
         StressPairs P;
         std::memset(&P, 0, sizeof(P));
         P.n = (int)std::min<size_t>(kStressPairs, pairs.size() - c0);
         for (int p = 0; p < P.n; p++) {
-            const Pr &q = pairs[c0 + p];
+            const StressPr &q = pairs[c0 + p];
             P.xs[p] = q.xs;
             P.xf[p] = q.xf;
             P.ys[p] = q.ys;
@@ -1277,32 +1302,41 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
             P.sel[p] = q.sel;
         }
         int nl;
-        if (T == 4) {
-            StressArgs<float> a{g, slot, (const float *)ctx->hist, (const float *)ctx->etab,
+        if (ctx->prec == SCFT_FP32) {
+            StressArgs<float> a{g, slot, (const float *)hist, (const float *)ctx->etab,
                                 (const cplx<float> *)ctx->tw, (const float *)ctx->kfac,
                                 (cplx<float> *)ctx->st_S4, (cplx<float> *)ctx->st_S2,
                                 (cplx<float> *)ctx->st_S4p, ctx->st_part,
                                 {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, (float)(1.0 / g.M), ctx->err};
+            a.jtab = (const float *)ctx->jtab;
             nl = launch_stress_chunk<float>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
                                             ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
         } else {
-            StressArgs<double> a{g, slot, (const double *)ctx->hist, (const double *)ctx->etab,
+            StressArgs<double> a{g, slot, (const double *)hist, (const double *)ctx->etab,
                                  (const cplx<double> *)ctx->tw, (const double *)ctx->kfac,
                                  (cplx<double> *)ctx->st_S4, (cplx<double> *)ctx->st_S2,
                                  (cplx<double> *)ctx->st_S4p, ctx->st_part,
                                  {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, 1.0 / g.M, ctx->err};
+            a.jtab = (const double *)ctx->jtab;
             nl = launch_stress_chunk<double>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
                                              ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
         }
         ctx->stats.kernel_launches += nl;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out.data(), ctx->st_out, sizeof(double) * 3 * P.n, cudaMemcpyDeviceToHost, ctx->st));
-        s = check_device_err(ctx);
+        scft_status s = check_device_err(ctx);
         if (s != SCFT_OK) return s;
         for (int p = 0; p < P.n; p++)
             for (int i = 0; i < 3; i++) (pairs[c0 + p].homo ? dQ2 : dQC)[i] += out[3 * p + i];
     }
-    const double invM = 1.0 / g.M, phic = ctx->p.phidb, alpha = ctx->p.alpha;
+    return SCFT_OK;
+}
+
+// d lnQ/dL from the pair sums (the ensemble's lnQ, density.h:388-399)
+void stress_finish(const scft_ctx *ctx, double Q2, double QC, double *dQC, double *dQ2, double *dlnQ_dL,
+                   double *dF_dL)
+{
+    const double invM = 1.0 / ctx->g.M, phic = ctx->p.phidb, alpha = ctx->p.alpha;
     for (int i = 0; i < 3; i++) {
         dQC[i] *= invM;
         dQ2[i] *= invM;
@@ -1314,6 +1348,285 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
         if (dlnQ_dL) dlnQ_dL[i] = d;
         if (dF_dL) dF_dL[i] = -d;
     }
+}
+
+// E table of q's step s (0 A, 1 B, 2 junction step of a continuous A fraction)
+int q_table(const Geo &g, int s) { return (g.jon && s == g.jq) ? 2 : (s < g.n1 ? 0 : 1); }
+
+// Symmetric partition of [0, n) into pieces of at most K steps: boundaries
+// 0, K, 2K, ... up to the middle and their mirrors n - jK, so that the mirror
+// [n-b, n-a) of every piece [a, b) is a piece too.
+std::vector<int> mirror_bounds(int n, int K)
+{
+    std::vector<int> b;
+    const int j = n / (2 * K), a = j * K, m = n - 2 * a;
+    for (int x = 0; x <= a; x += K) b.push_back(x);
+    if (m > K) {
+        if (m % 2 == 0) {
+            b.push_back(a + m / 2);
+        } else {
+            b.push_back(a + (m - 1) / 2);
+            b.push_back(a + (m + 1) / 2);
+        }
+    }
+    for (int x = a; x >= 0; x -= K) b.push_back(n - x);
+    std::sort(b.begin(), b.end());
+    b.erase(std::unique(b.begin(), b.end()), b.end());
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    scft_status s = stress_alloc(ctx);
+    if (s != SCFT_OK) return s;
+    // fresh propagators of replica ii
+    s = props_list(ctx, {ii});
+    if (s != SCFT_OK) return s;
+    const int slot = ctx->slot_of[ii];
+    const double Q2 = rsv(ctx, ii, kRsQ2), QC = rsv(ctx, ii, kRsQC);
+    // pairs: copolymer (q(s), q^dagger(N-1-s)), homopolymer (q^dagger(j), q^dagger(Nh-1-j))
+    std::vector<StressPr> pairs;
+    for (int s2 = 0; s2 < g.Ns; s2++) pairs.push_back({s2, 0, g.Ns - 1 - s2, 1, q_table(g, s2), 0});
+    for (int j = 0; j < g.Nh; j++) pairs.push_back({j, 1, g.Nh - 1 - j, 1, 1, 1});
+    double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
+    s = stress_pairs(ctx, slot, ctx->hist, pairs, dQC, dQ2);
+    if (s != SCFT_OK) return s;
+    stress_finish(ctx, Q2, QC, dQC, dQ2, dlnQ_dL, dF_dL);
+    return SCFT_OK;
+}
+
+// The same adjoint with the propagators stored only at checkpoints.
+// Positions: the starts of a mirror-symmetric partition of [0, N) into pieces
+// of at most K steps (and of [0, Nh) for the homopolymer pairs).  A forward
+// pass over the whole chain keeps those slices plus q(N) and q^dagger(Nh)
+// (for QC and Q2).  Then each piece [a, b) is recomputed together with its
+// mirror [N-b, N-a): the two segments hold q(s) and q^dagger(N-1-s) for every
+// s of both pieces, i.e. all of their pairs.  Cost: two chain passes; memory:
+// (#checkpoints + 2 (K+1) + 2) slice pairs instead of N+1.  The slices are the
+// same bits as the full store's (same kernels, same inputs), so the result
+// equals scft_stress up to the order of the final FP64 pair sums.
+scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL, double *bytes_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || K < 1) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    const int N = g.Ns, Nh = g.Nh;
+    K = std::min(K, N);
+    scft_status s = stress_alloc(ctx);
+    if (s != SCFT_OK) return s;
+    const std::vector<int> bc = mirror_bounds(N, K);
+    const std::vector<int> bh = Nh > 0 ? mirror_bounds(Nh, std::min(K, Nh)) : std::vector<int>{0};
+    // checkpoint rows: every piece start of both partitions
+    std::vector<int> row_of(N + 1, -1), pos;
+    for (size_t k = 0; k + 1 < bc.size(); k++) pos.push_back(bc[k]);
+    for (size_t k = 0; k + 1 < bh.size(); k++) pos.push_back(bh[k]);
+    std::sort(pos.begin(), pos.end());
+    pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
+    for (size_t r = 0; r < pos.size(); r++) row_of[pos[r]] = (int)r;
+    const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    const size_t pairB = 2 * (size_t)g.M * T;  // one slice pair (q, q^dagger)
+    const size_t nrow = pos.size() + 2 * (size_t)(K + 1) + 2;
+    const size_t need = nrow * pairB;
+    if (ctx->ck_bytes < need) {
+        if (ctx->ck_mem) cudaFree(ctx->ck_mem);
+        ctx->ck_mem = nullptr;
+        ctx->ck_bytes = 0;
+        CK(cudaMalloc(&ctx->ck_mem, need));
+        ctx->ck_bytes = need;
+    }
+    unsigned char *ck = (unsigned char *)ctx->ck_mem;        // [pos.size()] checkpoint pairs
+    unsigned char *seg = ck + pos.size() * pairB;             // segment A (K+1), segment B (K+1)
+    unsigned char *segB = seg + (size_t)(K + 1) * pairB;
+    unsigned char *qb = segB + (size_t)(K + 1) * pairB;       // [q^dagger(Nh) pair, q(N) pair]
+    if (bytes_out) *bytes_out = (double)need;
+
+    s = upload_list(ctx, {ii});
+    if (s != SCFT_OK) return s;
+    for (auto &so : ctx->slot_of)  // slot 0's E tables and spectra are reused below
+        if (so == 0) so = -1;
+    const bool f32 = ctx->prec == SCFT_FP32;
+    auto args_f = [&](Geo gg, void *hist) {
+        PropsArgs<float> a = props_args_from<float>(ctx, ctx->rep_dev, 0);
+        a.g = gg;
+        a.hist = (float *)hist;
+        return a;
+    };
+    auto args_d = [&](Geo gg, void *hist) {
+        PropsArgs<double> a = props_args_from<double>(ctx, ctx->rep_dev, 0);
+        a.g = gg;
+        a.hist = (double *)hist;
+        return a;
+    };
+    auto chain = [&](int p0, int len, void *buf, int first_mode) {
+        Geo gg = g;
+        gg.Ns = len;
+        gg.n1 = g.n1 - p0;
+        gg.n2 = g.n2 - p0;
+        gg.jq = g.jq - p0;
+        gg.jqd = g.jqd - p0;
+        ctx->stats.kernel_launches += f32 ? launch_chain<float>(args_f(gg, buf), ctx->L, first_mode, ctx->st)
+                                          : launch_chain<double>(args_d(gg, buf), ctx->L, first_mode, ctx->st);
+    };
+    auto cp = [&](void *dst, const void *src) {
+        return cudaMemcpyAsync(dst, src, pairB, cudaMemcpyDeviceToDevice, ctx->st);
+    };
+    // forward pass: E tables of replica ii in slot 0, then the chain piece by piece
+    ctx->stats.kernel_launches += f32 ? launch_prepare<float>(args_f(g, ctx->hist), ctx->L, ctx->st)
+                                      : launch_prepare<double>(args_d(g, ctx->hist), ctx->L, ctx->st);
+    std::vector<int> stops(pos);
+    stops.push_back(N);
+    if (Nh > 0 && Nh < N) stops.push_back(Nh);
+    std::sort(stops.begin(), stops.end());
+    stops.erase(std::unique(stops.begin(), stops.end()), stops.end());
+    int prev = 0;  // length of the previous piece: its last slice starts the next one
+    for (size_t k = 0; k + 1 < stops.size(); k++) {
+        const int p0 = stops[k], p1 = stops[k + 1];
+        if (p0 > 0) CK(cp(seg, seg + (size_t)prev * pairB));
+        chain(p0, p1 - p0, seg, p0 == 0 ? 1 : 2);
+        prev = p1 - p0;
+        if (p0 == 0) CK(cp(ck + row_of[0] * pairB, seg));
+        if (p0 == 0 && Nh == 0) CK(cp(qb, seg));
+        if (p1 < N && row_of[p1] >= 0) CK(cp(ck + row_of[p1] * pairB, seg + (size_t)(p1 - p0) * pairB));
+        if (p1 == Nh) CK(cp(qb, seg + (size_t)(p1 - p0) * pairB));
+        if (p1 == N) CK(cp(qb + pairB, seg + (size_t)(p1 - p0) * pairB));
+    }
+    CK(cudaGetLastError());
+    // Q2 = <q^dagger(Nh)>, QC = <q(N)>: a two-slice store with Ns = 1, Nh = 0
+    {
+        Geo gq = g;
+        gq.Ns = 1;
+        gq.Nh = 0;
+        ctx->stats.kernel_launches += f32 ? launch_qsums<float>(args_f(gq, qb), ctx->L, ctx->st)
+                                          : launch_qsums<double>(args_d(gq, qb), ctx->L, ctx->st);
+        CK(cudaMemcpyAsync(&ctx->rs_h[(size_t)ii * kRsStride], ctx->rs + (size_t)ii * kRsStride,
+                           sizeof(double) * kRsStride, cudaMemcpyDeviceToHost, ctx->st));
+        s = check_device_err(ctx);
+        if (s != SCFT_OK) return s;
+    }
+    const double Q2 = rsv(ctx, ii, kRsQ2), QC = rsv(ctx, ii, kRsQC);
+    double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
+    // recompute each piece with its mirror; the pairs of both pieces
+    auto sweep = [&](const std::vector<int> &b, int n, bool homo) -> scft_status {
+        const size_t segoff = (size_t)(K + 1);  // slice index of segment B's first slice
+        for (size_t k = 0; k + 1 < b.size(); k++) {
+            const int a0 = b[k], a1 = b[k + 1], m0 = n - a1, m1 = n - a0;
+            if (a0 > m0) continue;  // right half: done as a mirror
+            const bool self = (a0 == m0);
+            std::vector<StressPr> pairs;
+            cudaError_t e = cp(seg, ck + row_of[a0] * pairB);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "checkpoint copy");
+            chain(a0, a1 - a0, seg, 2);
+            if (!self) {
+                e = cp(segB, ck + row_of[m0] * pairB);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "checkpoint copy");
+                chain(m0, m1 - m0, segB, 2);
+            }
+            const int yb = self ? 0 : (int)segoff;  // where the mirror piece's slices are
+            // pairs (x(t), y(n-1-t)) for t in [a0, a1): x in segment A, y in the mirror
+            for (int t = a0; t < a1; t++) {
+                const int u = n - 1 - t;
+                if (homo)
+                    pairs.push_back({t - a0, 1, yb + (u - m0), 1, 1, 1});
+                else
+                    pairs.push_back({t - a0, 0, yb + (u - m0), 1, q_table(g, t), 0});
+            }
+            if (!self)
+                for (int t = m0; t < m1; t++) {
+                    const int u = n - 1 - t;
+                    if (homo)
+                        pairs.push_back({(int)segoff + (t - m0), 1, u - a0, 1, 1, 1});
+                    else
+                        pairs.push_back({(int)segoff + (t - m0), 0, u - a0, 1, q_table(g, t), 0});
+                }
+            scft_status st = stress_pairs(ctx, 0, seg, pairs, dQC, dQ2);
+            if (st != SCFT_OK) return st;
+        }
+        return SCFT_OK;
+    };
+    s = sweep(bc, N, false);
+    if (s != SCFT_OK) return s;
+    if (Nh > 0) {
+        s = sweep(bh, Nh, true);
+        if (s != SCFT_OK) return s;
+    }
+    stress_finish(ctx, Q2, QC, dQC, dQ2, dlnQ_dL, dF_dL);
+    return SCFT_OK;
+}
+
+// d lnQ/df of replica ii at its current fields with a continuous A fraction
+// (fcont): f moves the junction inside q's step n1 = floor(N f), whose field is
+// theta wA + (1-theta) wB with theta = N f - n1, so d/df = N d/dtheta and only
+// QC depends on f:  dQC/dtheta = (1/M) <q^dagger(N-1-n1), dS_J/dtheta q(n1)>
+// (the adjoint of the junction step, stress_kernels.cu).  dF/df = -d lnQ/df
+// at a converged saddle point.
+scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    if (!g.jon) {
+        ctx->lasterr = "scft_dF_df: needs a continuous A fraction (scft_problem.fcont = 1)";
+        return SCFT_BAD_INPUT;
+    }
+    scft_status s = stress_alloc(ctx);
+    if (s != SCFT_OK) return s;
+    const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    if (!ctx->jd_rbuf) CK(cudaMalloc(&ctx->jd_rbuf, T * 6 * (size_t)g.M));
+    s = props_list(ctx, {ii});
+    if (s != SCFT_OK) return s;
+    const int slot = ctx->slot_of[ii];
+    const double QC = rsv(ctx, ii, kRsQC), zC = rsv(ctx, ii, kRsZC);
+    StressPairs P;
+    std::memset(&P, 0, sizeof(P));
+    P.n = 1;
+    P.xs[0] = g.n1;                  // q(n1), the junction step's input
+    P.xf[0] = 0;
+    P.ys[0] = g.Ns - 1 - g.n1;       // q^dagger(N-1-n1), its adjoint
+    P.yf[0] = 1;
+    P.sel[0] = 2;
+    const double *wm = ctx->W + (size_t)ii * 2 * ctx->M;
+    int nl;
+    if (T == 4) {
+        StressArgs<float> a{g, slot, (const float *)ctx->hist, (const float *)ctx->etab,
+                            (const cplx<float> *)ctx->tw, (const float *)ctx->kfac,
+                            (cplx<float> *)ctx->st_S4, (cplx<float> *)ctx->st_S2,
+                            (cplx<float> *)ctx->st_S4p, ctx->st_part,
+                            {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, (float)(1.0 / g.M), ctx->err};
+        a.jtab = (const float *)ctx->jtab;
+        a.rbuf = (float *)ctx->jd_rbuf;
+        a.wminus = wm;
+        nl = launch_junction_dtheta<float>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem, ctx->rt_pencil_threads,
+                                           ctx->rt_pencil_smem, ctx->partials, ctx->L.red_blocks, ctx->redout,
+                                           ctx->st);
+    } else {
+        StressArgs<double> a{g, slot, (const double *)ctx->hist, (const double *)ctx->etab,
+                             (const cplx<double> *)ctx->tw, (const double *)ctx->kfac,
+                             (cplx<double> *)ctx->st_S4, (cplx<double> *)ctx->st_S2,
+                             (cplx<double> *)ctx->st_S4p, ctx->st_part,
+                             {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, 1.0 / g.M, ctx->err};
+        a.jtab = (const double *)ctx->jtab;
+        a.rbuf = (double *)ctx->jd_rbuf;
+        a.wminus = wm;
+        nl = launch_junction_dtheta<double>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem, ctx->rt_pencil_threads,
+                                            ctx->rt_pencil_smem, ctx->partials, ctx->L.red_blocks, ctx->redout,
+                                            ctx->st);
+    }
+    ctx->stats.kernel_launches += nl;
+    CK(cudaGetLastError());
+    double sum = 0;
+    CK(cudaMemcpyAsync(&sum, ctx->redout, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    s = check_device_err(ctx);
+    if (s != SCFT_OK) return s;
+    const double dQC = sum / g.M;  // dQC/dtheta
+    // lnQ = phic ln QC + ... (ens 1, density.h:390); zB Q2 + zC QC (ens 2, density.h:398)
+    const double dth = ctx->p.ens == 1 ? ctx->p.phidb * dQC / QC : zC * dQC;
+    const double d = g.Ns * dth;
+    if (dlnQ_df) *dlnQ_df = d;
+    if (dF_df) *dF_df = -d;
     return SCFT_OK;
 }
 

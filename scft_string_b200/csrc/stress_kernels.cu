@@ -31,6 +31,13 @@ __device__ __forceinline__ const T *slice(const StressArgs<T> &a, int s, int fld
     return a.hist + (((size_t)a.slot * (a.g.Ns + 1) + s) * 2 + fld) * (size_t)a.g.M;
 }
 
+// E4 table `sel` (0 A, 1 B, 2 junction step) of the slot
+template <typename T>
+__device__ __forceinline__ const T *etab_of(const StressArgs<T> &a, int sel)
+{
+    return sel == 2 ? a.jtab + (size_t)a.slot * a.g.M : a.etab + ((size_t)a.slot * 2 + sel) * a.g.M;
+}
+
 __device__ __forceinline__ double bsum(double v, double *sh)
 {
 #pragma unroll
@@ -60,7 +67,7 @@ __global__ void k_stress_slab_fwd(StressArgs<T> a, StressPairs P)
     const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
     const T *src = slice(a, xy ? P.ys[p] : P.xs[p], xy ? P.yf[p] : P.xf[p]) + slab_r;
-    const T *E4 = a.etab + ((size_t)a.slot * 2 + P.sel[p]) * g.M + slab_r;
+    const T *E4 = etab_of(a, P.sel[p]) + slab_r;
     const int npz = g.npair * m2;
     for (int pass = 0; pass < 2; pass++) {
         __syncthreads();
@@ -182,7 +189,7 @@ __global__ void k_stress_slab_mid(StressArgs<T> a, StressPairs P)
     const int x = blockIdx.x, xy = blockIdx.y, p = blockIdx.z;
     const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
-    const T *E4 = a.etab + ((size_t)a.slot * 2 + P.sel[p]) * g.M + slab_r;
+    const T *E4 = etab_of(a, P.sel[p]) + slab_r;
     cplx<T> *sp = a.S4p + ((size_t)p * 2 + xy) * g.Mk + slab_k;
     for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = sp[i];
     __syncthreads();
@@ -263,7 +270,177 @@ __global__ void k_stress_final(const double *part, int ntiles, int npairs, doubl
     out[p * 3 + i] = invM * (4.0 / 3.0 * t12 - 1.0 / 3.0 * t3);
 }
 
+// ---------------------------------------------------------------- junction step
+// d/dtheta of q's junction step with a continuous A fraction.  The step is
+// S = (4 E4 D2 E2 D2 E4 - E2 D1 E2)/3 with the field theta wA + (1-theta) wB,
+// so dE4/dtheta = -(ds/4) delta E4, dE2/dtheta = -(ds/2) delta E2 with
+// delta = wA - wB = 2 W-.  With b = D2 E4 v, d = D2 E2 b, g = D1 E2 v
+// (v = x, y; D symmetric, E diagonal):
+//   <y, dS/dtheta x> = -(ds/3) sum delta (y E4 d_x + d_y E4 x)
+//                      -(2 ds/3) sum delta b_y E2 b_x
+//                      +(ds/6) sum delta (y E2 g_x + g_y E2 x)
+// Launches: k_stress_slab_fwd (spectra of E4 v, E2 v), pencil pass 0 (K2 on
+// the first, K1 on the second), slab pass 0 (b, g real; spectrum of E2 b),
+// pencil pass 1 (K2), slab pass 1 (d real), reduction.
+// rbuf rows: 0 b_x, 1 b_y, 2 g_x, 3 g_y, 4 d_x, 5 d_y.
+
+// x transform of a column tile, times K2/M (k1 = 0) or K1/M (k1 = 1), back
+template <typename T>
+__device__ void jn_pencil_tile(const StressArgs<T> &a, cplx<T> *bx, const cplx<T> *twx, const cplx<T> *src,
+                               cplx<T> *dst, int c0, int k1)
+{
+    const Geo &g = a.g;
+    const int tc = g.tc, m0 = g.m0, ncol = g.m1 * g.mk2;
+    __syncthreads();
+    for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        const int xx = e / tc, t = e - xx * tc, c = c0 + t;
+        bx[e] = c < ncol ? src[(size_t)xx * ncol + c] : cplx<T>{(T)0, (T)0};
+    }
+    __syncthreads();
+    cta_fft(bx, g.px, tc, tc, 1, true, twx, -1, a.err);
+    for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        const int xx = e / tc, t = e - xx * tc, c = c0 + t;
+        const int yk = c / g.mk2, kz = c - yk * g.mk2;
+        T f = (T)0;
+        if (c < ncol) {
+            const T k = a.kfac[xx] * a.kfac[m0 + yk] * a.kfac[m0 + g.m1 + kz];
+            f = (k1 ? k * k : k) * a.invM;
+        }
+        bx[e].x *= f;
+        bx[e].y *= f;
+    }
+    __syncthreads();
+    cta_fft(bx, g.px, tc, tc, 1, true, twx, +1, a.err);
+    for (int e = threadIdx.x; e < tc * m0; e += blockDim.x) {
+        const int xx = e / tc, t = e - xx * tc, c = c0 + t;
+        if (c < ncol) dst[(size_t)xx * ncol + c] = bx[e];
+    }
+}
+
+template <typename T>
+__global__ void k_jn_pencil(StressArgs<T> a, int pass)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const Geo &g = a.g;
+    cplx<T> *bx = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *twx = bx + g.tc * g.m0;
+    for (int i = threadIdx.x; i < g.m0; i += blockDim.x) twx[i] = a.tw[i];
+    const int tile = blockIdx.x, xy = blockIdx.y, c0 = tile * g.tc;
+    cplx<T> *s4 = a.S4 + (size_t)xy * g.Mk, *s4p = a.S4p + (size_t)xy * g.Mk, *s2 = a.S2 + (size_t)xy * g.Mk;
+    jn_pencil_tile(a, bx, twx, s4, s4p, c0, 0);
+    if (pass == 0) jn_pencil_tile(a, bx, twx, s2, s2, c0, 1);
+}
+
+// inverse slab transform of `src` into the real slab `dst` (slab_r offset applied)
+template <typename T>
+__device__ void jn_slab_to_real(const StressArgs<T> &a, cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz,
+                                const cplx<T> *src, T *dst)
+{
+    const Geo &g = a.g;
+    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2;
+    __syncthreads();
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) buf[i] = src[i];
+    __syncthreads();
+    slab_inverse(buf, g, twy, twz, a.err);
+    for (int e = threadIdx.x; e < g.npair * m2; e += blockDim.x) {
+        const int pp = e / m2, z = e - pp * m2;
+        const cplx<T> c = buf[2 * pp * mk2 + z];
+        const int r0 = 2 * pp * m2 + z;
+        dst[r0] = c.x;
+        if (2 * pp + 1 < m1) dst[r0 + m2] = c.y;
+    }
+}
+
+template <typename T>
+__global__ void k_jn_slab(StressArgs<T> a, int pass)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const Geo &g = a.g;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *twy = buf + g.slab_c;
+    cplx<T> *twz = twy + g.m1;
+    for (int i = threadIdx.x; i < g.m1; i += blockDim.x) twy[i] = a.tw[g.m0 + i];
+    for (int i = threadIdx.x; i < g.m2; i += blockDim.x) twz[i] = a.tw[g.m0 + g.m1 + i];
+    const int x = blockIdx.x, xy = blockIdx.y;
+    const int m1 = g.m1, m2 = g.m2, mk2 = g.mk2;
+    const size_t M = g.M, slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
+    cplx<T> *s4 = a.S4 + (size_t)xy * g.Mk + slab_k, *s4p = a.S4p + (size_t)xy * g.Mk + slab_k;
+    cplx<T> *s2 = a.S2 + (size_t)xy * g.Mk + slab_k;
+    if (pass == 1) {
+        jn_slab_to_real(a, buf, twy, twz, s4p, a.rbuf + (4 + xy) * M + slab_r);  // d
+        return;
+    }
+    T *b = a.rbuf + (0 + xy) * M + slab_r;
+    jn_slab_to_real(a, buf, twy, twz, s4p, b);                                  // b = D2 E4 v
+    const T *E4 = etab_of(a, 2) + slab_r;
+    __syncthreads();
+    for (int e = threadIdx.x; e < g.npair * m2; e += blockDim.x) {
+        const int pp = e / m2, z = e - pp * m2;
+        const int r0 = 2 * pp * m2 + z;
+        const T e0 = E4[r0];
+        T v1 = (T)0;
+        if (2 * pp + 1 < m1) {
+            const T e1 = E4[r0 + m2];
+            v1 = b[r0 + m2] * (e1 * e1);
+        }
+        buf[2 * pp * mk2 + z] = {b[r0] * (e0 * e0), v1};
+    }
+    __syncthreads();
+    slab_forward(buf, g, twy, twz, a.err);                                      // spectrum of E2 b
+    for (int i = threadIdx.x; i < m1 * mk2; i += blockDim.x) s4[i] = buf[i];
+    jn_slab_to_real(a, buf, twy, twz, s2, a.rbuf + (2 + xy) * M + slab_r);      // g = D1 E2 v
+}
+
+template <typename T>
+__global__ void k_jn_reduce(StressArgs<T> a, StressPairs P, double *part)
+{
+    __shared__ double sh[32];
+    const Geo &g = a.g;
+    const size_t M = g.M;
+    const T *x = slice(a, P.xs[0], P.xf[0]), *y = slice(a, P.ys[0], P.yf[0]);
+    const T *E4 = etab_of(a, 2);
+    const T *bx = a.rbuf, *by = a.rbuf + M, *gx = a.rbuf + 2 * M, *gy = a.rbuf + 3 * M;
+    const T *dx = a.rbuf + 4 * M, *dy = a.rbuf + 5 * M;
+    const double ds = 1.0 / g.Ns;
+    double acc = 0;
+    for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += (size_t)gridDim.x * blockDim.x) {
+        const double del = 2.0 * a.wminus[r];
+        const double e4 = (double)E4[r], e2 = e4 * e4;
+        const double X = x[r], Y = y[r];
+        const double t1 = Y * e4 * (double)dx[r] + (double)dy[r] * e4 * X;
+        const double t2 = (double)by[r] * e2 * (double)bx[r];
+        const double t3 = Y * e2 * (double)gx[r] + (double)gy[r] * e2 * X;
+        acc += del * (-(ds / 3.0) * t1 - (2.0 * ds / 3.0) * t2 + (ds / 6.0) * t3);
+    }
+    const double t = bsum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_jn_final(const double *part, int nblk, double *out)
+{
+    if (threadIdx.x != 0) return;
+    double t = 0;
+    for (int i = 0; i < nblk; i++) t += part[i];
+    out[0] = t;
+}
+
 }  // namespace
+
+template <typename T>
+int launch_junction_dtheta(const StressArgs<T> &a, const StressPairs &P, int slab_threads, int slab_smem,
+                           int pencil_threads, int pencil_smem, double *part, int nblk, double *out,
+                           cudaStream_t st)
+{
+    const Geo &g = a.g;
+    k_stress_slab_fwd<T><<<dim3(g.m0, 2, 1), slab_threads, slab_smem, st>>>(a, P);
+    k_jn_pencil<T><<<dim3(g.ncol_tiles, 2), pencil_threads, pencil_smem, st>>>(a, 0);
+    k_jn_slab<T><<<dim3(g.m0, 2), slab_threads, slab_smem, st>>>(a, 0);
+    k_jn_pencil<T><<<dim3(g.ncol_tiles, 2), pencil_threads, pencil_smem, st>>>(a, 1);
+    k_jn_slab<T><<<dim3(g.m0, 2), slab_threads, slab_smem, st>>>(a, 1);
+    k_jn_reduce<T><<<nblk, 256, 0, st>>>(a, P, part);
+    k_jn_final<<<1, 32, 0, st>>>(part, nblk, out);
+    return 7;
+}
 
 template <typename T>
 int launch_stress_chunk(const StressArgs<T> &a, const StressPairs &P, int slab_threads, int slab_smem,
@@ -285,11 +462,18 @@ int set_stress_smem(int slab_smem, int pencil_smem)
     cudaError_t e2 = cudaFuncSetAttribute(k_stress_slab_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem);
     cudaError_t e3 = cudaFuncSetAttribute(k_stress_pencil1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
     cudaError_t e4 = cudaFuncSetAttribute(k_stress_pencil2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
-    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess) ? 0 : -1;
+    cudaError_t e5 = cudaFuncSetAttribute(k_jn_slab<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem);
+    cudaError_t e6 = cudaFuncSetAttribute(k_jn_pencil<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess &&
+            e5 == cudaSuccess && e6 == cudaSuccess) ? 0 : -1;
 }
 
 template int launch_stress_chunk<float>(const StressArgs<float> &, const StressPairs &, int, int, int, int, double *, cudaStream_t);
 template int launch_stress_chunk<double>(const StressArgs<double> &, const StressPairs &, int, int, int, int, double *, cudaStream_t);
+template int launch_junction_dtheta<float>(const StressArgs<float> &, const StressPairs &, int, int, int, int,
+                                           double *, int, double *, cudaStream_t);
+template int launch_junction_dtheta<double>(const StressArgs<double> &, const StressPairs &, int, int, int, int,
+                                            double *, int, double *, cudaStream_t);
 template int set_stress_smem<float>(int, int);
 template int set_stress_smem<double>(int, int);
 

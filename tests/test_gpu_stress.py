@@ -111,3 +111,36 @@ def test_variable_cell_relaxation_lowers_stress(built_lib):
     print("rounds", n, "stress", st, "box", box, "initial stress", s0)
     assert np.abs(st).max() <= 1e-6
     assert abs(box[0] - D[0]) < 1e-12 and abs(box[1] - D[1]) < 1e-12  # no x, y structure: no stress
+
+
+@pytest.mark.parametrize("m,D,N,ens,K,prec", [
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 1, 1, "fp64"),     # every slice a checkpoint
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 1, 3, "fp64"),     # K does not divide N
+    ((12, 8, 16), (3.1, 2.2, 4.0), 24, 2, 5, "fp64"),
+    ((12, 8, 16), (3.1, 2.2, 4.0), 24, 2, 100, "fp64"),   # one segment
+    ((32, 32, 32), (4.0, 4.0, 4.0), 40, 1, 6, "fp64"),    # compile-time shape
+    ((32, 32, 32), (4.0, 4.0, 4.0), 101, 1, 7, "fp32"),   # odd middle piece
+    ((64, 64, 96), (4.2, 4.2, 6.3), 160, 1, 13, "fp32"),  # 64x64x96, N=160, every 13 steps
+])
+def test_checkpointed_adjoint_equals_full_store(built_lib, m, D, N, ens, K, prec):
+    """The adjoint with propagators kept every K contour steps (recomputed in
+    mirrored segment pairs) gives the full-store adjoint's values: the
+    recomputed slices are the same bits, only the FP64 pair sums are added in
+    another order."""
+    D = np.array(D)
+    wm, wp = smooth_fields(m, D, 2)
+    ctx = S.Context(m, D, N, chi=12, f=0.45, phidb=0.8, ens=ens, alpha=0.1, strn=1, dostring=0,
+                    precision=prec)
+    ctx.set_fields(0, wm, wp)
+    full, _ = ctx.stress(0)
+    ck, dF, nbytes = ctx.stress_ckpt(0, K)
+    assert np.allclose(dF, -ck)
+    tol = 1e-11 * np.abs(full).max()
+    assert np.abs(ck - full).max() <= tol, (ck, full)
+    store = (N + 1) * 2 * ctx.M * (4 if prec == "fp32" else 8)
+    if 3 <= K < N:
+        assert nbytes < store
+    print(m, N, K, prec, "checkpointed bytes", nbytes, "full store", store)
+    # the full-store path still works after the checkpointed one reused slot 0
+    again, _ = ctx.stress(0)
+    np.testing.assert_array_equal(again, full)

@@ -168,7 +168,8 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
 /* Anderson-accelerated solution of replica ii's field equations (an option
  * beside the reference's simple mixing; no reference counterpart): residual
  * as scft.cu:605-607 without spring or string terms, history of nhist
- * (1..30) iterates, FP64 least squares, mixing parameter lam.  Stops when the
+ * (1..30) iterates restarted every 16 nhist iterations, FP64 least squares,
+ * mixing parameter lam.  Stops when the
  * RMS residual <= tol; *iters = props evaluations, *err_out = last RMS. */
 scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, int nhist, double lam,
                                 int *iters, double *err_out);

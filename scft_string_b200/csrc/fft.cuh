@@ -395,6 +395,105 @@ __device__ __forceinline__ void fft_fixed(cplx<T> *buf, const cplx<T> *tw, int s
     }
 }
 
+// Radix schedule of the fixed transforms: greedy 8, 4, 2, 3, 5, 7.
+template <int N>
+struct RadixPlan {
+    __host__ __device__ static constexpr int stages()
+    {
+        int s = 0, ns = 1;
+        while (ns < N) {
+            ns *= pick_radix(N / ns);
+            s++;
+        }
+        return s;
+    }
+    __host__ __device__ static constexpr int radix(int i)
+    {
+        int ns = 1;
+        for (int k = 0; k < i; k++) ns *= pick_radix(N / ns);
+        return pick_radix(N / ns);
+    }
+    __host__ __device__ static constexpr int rradix(int i) { return radix(stages() - 1 - i); }  // reversed schedule
+};
+
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, int SIGN, int I, int NS>
+__device__ __forceinline__ void stages_but_last(cplx<T> *buf, const cplx<T> *tw)
+{
+    if constexpr (I < RadixPlan<N>::stages() - 1) {
+        constexpr int R = RadixPlan<N>::radix(I);
+        fft_stage_fixed<T, N, NLINES, ES, LS, LF, NT, R, NS>(buf, tw, SIGN);
+        stages_but_last<T, N, NLINES, ES, LS, LF, NT, SIGN, I + 1, NS * R>(buf, tw);
+    }
+}
+
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, int SIGN, int I, int NS>
+__device__ __forceinline__ void stages_reversed(cplx<T> *buf, const cplx<T> *tw)
+{
+    if constexpr (I < RadixPlan<N>::stages()) {
+        constexpr int R = RadixPlan<N>::rradix(I);
+        fft_stage_fixed<T, N, NLINES, ES, LS, LF, NT, R, NS>(buf, tw, SIGN);
+        stages_reversed<T, N, NLINES, ES, LS, LF, NT, SIGN, I + 1, NS * R>(buf, tw);
+    }
+}
+
+// Transform (sign SIGN), pointwise multiply, transform back (sign -SIGN) of
+// NLINES lines in place.  Butterfly j of the first transform's last stage
+// (radix R) holds the outputs j + r N/R, which are exactly the inputs of
+// butterfly j of the first stage of a transform that runs the radices in
+// reverse order; so those two stages and the multiply run in registers with
+// one shared-memory round trip instead of three.  mul(v, line, k) scales
+// element k of line `line`.
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, int SIGN, class Mul>
+__device__ __forceinline__ void fft_pair_fused(cplx<T> *__restrict__ buf, const cplx<T> *__restrict__ tw, Mul mul)
+{
+    stages_but_last<T, N, NLINES, ES, LS, LF, NT, SIGN, 0, 1>(buf, tw);
+    constexpr int R = RadixPlan<N>::radix(RadixPlan<N>::stages() - 1);
+    constexpr int NR = N / R;  // also the stride NS of the first transform's last stage
+    constexpr int NB = NLINES * NR;
+    constexpr int PER = (NB + NT - 1) / NT;
+    cplx<T> v[PER][R];
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+            const cplx<T> *src = buf + line * LS + j * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                cplx<T> a = src[r * NR * ES];
+                if (NR > 1 && r > 0) a = SIGN < 0 ? cmul(a, tw[r * j]) : cmulc(a, tw[r * j]);
+                v[i][r] = a;
+            }
+            Dft<T, R>::run(v[i], SIGN, tw, N);
+#pragma unroll
+            for (int r = 0; r < R; r++) mul(v[i][r], line, j + r * NR);
+            Dft<T, R>::run(v[i], -SIGN, tw, N);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+            cplx<T> *dst = buf + line * LS + j * R * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[r * ES] = v[i][r];
+        }
+    }
+    __syncthreads();
+    stages_reversed<T, N, NLINES, ES, LS, LF, NT, -SIGN, 1, RadixPlan<N>::rradix(0)>(buf, tw);
+}
+
+// forward transform, multiply, inverse transform
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, class Mul>
+__device__ __forceinline__ void fft_fwd_mul_inv(cplx<T> *buf, const cplx<T> *tw, Mul mul)
+{
+    fft_pair_fused<T, N, NLINES, ES, LS, LF, NT, -1>(buf, tw, mul);
+}
+
 // Packed z-rows of the fixed shapes sit at an odd stride of M2 + 1 complex
 // elements, so that a warp transforming 32 rows at once (lines fastest) reads
 // and writes 32 different banks; the half spectra [y][kz] keep their natural

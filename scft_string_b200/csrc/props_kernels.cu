@@ -585,17 +585,15 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     for (int pass = 0; pass < npass; pass++) {
         cplx<T> *buf = pass == 0 ? bufA : bufB;
         mbar_wait(&bars[pass], 0, a.err);
-        fft_fixed<T, m0, TC, TC, 1, true, MT>(buf, twx, -1);
-        for (int e = threadIdx.x; e < BOX; e += MT) {
-            const int xx = e / TC, t = e - xx * TC;
+        // x forward, times the diffusion factor, x inverse; bin xx of column t:
+        // pass 0: K2 = g/M ; pass 1: K1 = g^2/M  (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
+        const T Mreal = a.Mreal;
+        fft_fwd_mul_inv<T, m0, TC, TC, 1, true, MT>(buf, twx, [&](cplx<T> &v, int t, int xx) {
             const T k2 = gx[xx] * colf[t];
-            // pass 0: K2 = g/M ; pass 1: K1 = g^2/M  (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
-            const T f = pass == 0 ? k2 * invM : (k2 * invM) * (k2 * invM) * a.Mreal;
-            buf[e].x *= f;
-            buf[e].y *= f;
-        }
-        __syncthreads();
-        fft_fixed<T, m0, TC, TC, 1, true, MT>(buf, twx, +1);
+            const T f = pass == 0 ? k2 * invM : (k2 * invM) * (k2 * invM) * Mreal;
+            v.x *= f;
+            v.y *= f;
+        });
         fence_proxy_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) tma_store_2d(&tmap, x, y0 + pass * m0, buf);
@@ -682,6 +680,32 @@ __device__ __forceinline__ void kahan_add(double &sum, double &c, double term)
     sum = t;
 }
 
+// sum += w_s u(s) v(t - s) for s in [s0, s1) with Simpson interior weights
+// 4, 2, 4, ... from s0 (the reference's loops, density.h:404-422), Kahan
+// compensated, in the reference's order.  u, v are fields fu, fv of the
+// propagator store at point r.  The loads of four consecutive terms are
+// issued before their additions, so each thread keeps eight loads in flight
+// instead of two.
+template <typename T>
+__device__ __forceinline__ void simpson_run(const T *h, size_t M, int r, int s0, int s1, int fu, int fv, int t,
+                                            double &sum, double &c)
+{
+    int s = s0;
+    for (; s + 3 < s1; s += 4) {
+        double u[4], v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            u[k] = (double)h[((size_t)(s + k) * 2 + fu) * M + r];
+            v[k] = (double)h[((size_t)(t - s - k) * 2 + fv) * M + r];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) kahan_add(sum, c, (((s + k - s0) & 1) ? 2 : 4) * u[k] * v[k]);
+    }
+    for (; s < s1; s++)
+        kahan_add(sum, c, (((s - s0) & 1) ? 2 : 4) * (double)h[((size_t)s * 2 + fu) * M + r] *
+                              (double)h[((size_t)(t - s) * 2 + fv) * M + r]);
+}
+
 // Composite-Simpson densities (rA_rB_init_Ns_homo, rA_rB_mid_segments,
 // scale_concentrations, sumconcs2: GPU_kernels.h:92-139; loops density.h:402-430).
 // Weights 1, 4, 2, 4, ... restart at 4 for each block with no odd-count
@@ -710,10 +734,9 @@ __global__ void k_density(PropsArgs<T> a)
         const double q12 = Q1(n1) * Q2(n2);
         double rCA = Q2(Ns) + q12, cA = 0;
         double rCB = Q1(Ns) + q12, cB = 0;
-        int s, wt;
-        for (s = 1, wt = 4; s < Nh; s++, wt = 6 - wt) kahan_add(rhB, chB, wt * Q2(s) * Q2(Nh - s));
-        for (s = 1, wt = 4; s < n1; s++, wt = 6 - wt) kahan_add(rCA, cA, wt * Q1(s) * Q2(Ns - s));
-        for (s = n1 + 1, wt = 4; s < Ns; s++, wt = 6 - wt) kahan_add(rCB, cB, wt * Q1(s) * Q2(Ns - s));
+        simpson_run(h, M, r, 1, Nh, 1, 1, Nh, rhB, chB);     // Q2(s) Q2(Nh - s)
+        simpson_run(h, M, r, 1, n1, 0, 1, Ns, rCA, cA);      // Q1(s) Q2(Ns - s)
+        simpson_run(h, M, r, n1 + 1, Ns, 0, 1, Ns, rCB, cB); // Q1(s) Q2(Ns - s)
         if (g.jon) {
             // continuous A fraction: theta of the junction step's trapezoid
             // weight moves from the B block to the A block (3/2 here: the sums

@@ -1635,7 +1635,8 @@ scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
 // scft.cu:30-31): residual d = (chi (phiB - phiA) - 2 W-, chi (phiA + phiB - 1))
 // as in scft.cu:605-607, history of up to nhist previous (W, d), least squares
 // in FP64 on the host over the device-computed Gram matrix of the residuals,
-// W <- (W_k + lam d_k) - sum_i theta_i ((W_k + lam d_k) - (W_i + lam d_i)).
+// W <- (W_k + lam d_k) - sum_i theta_i ((W_k + lam d_k) - (W_i + lam d_i)),
+// with the history restarted every 16 nhist iterations.
 scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, int nhist, double lam,
                                 int *iters, double *err_out)
 {
@@ -1671,6 +1672,9 @@ scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, 
         }
         if (err <= tol) break;
         const int k = it % H;
+        // restart: the history is cleared every 16 nhist iterations (a stale
+        // history stalls the extrapolation on slowly ordering 3-D states)
+        if (it > 0 && it % (16 * nhist) == 0) hist.clear();
         double *W = ctx->W + (size_t)ii * n2M;
         CK(cudaMemcpyAsync(ctx->and_X + (size_t)k * n2M, W, sizeof(double) * n2M, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->and_D + (size_t)k * n2M, ctx->DEV + (size_t)ii * n2M, sizeof(double) * n2M,

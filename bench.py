@@ -396,7 +396,7 @@ def run_ours(a, cfg, rank, world, dev):
     ctx = S.StringSolver(cfg, precision=a.precision, batched=not a.plain, device=dev)
     for ii in range(cfg["strn"]):
         ctx.set_fields(ii, wm[ii], wp[ii])
-    groups, tune_ms = ctx.autotune()           # 1 or 2 concurrent slot groups per props round
+    groups, wide, tune_ms = ctx.autotune()     # slot groups and pencil tile width per props round
     ctx.solve_field0_all(5000, 1e-4)           # prelude, scft.cu:1105
     nsterp = 4000                              # scft.cu:1102
     ctx.string_begin(nsterp, 1e-3)
@@ -431,7 +431,8 @@ def run_ours(a, cfg, rank, world, dev):
     e2e_ms = max_over_ranks(ctx.timer_elapsed_ms(2, 3))
     barrier()
     out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M,
-               schedule={"slot_groups": groups, "props_round_ms_by_groups": tune_ms})
+               schedule={"slot_groups": groups, "wide_pencil_tiles": bool(wide),
+                         "props_round_ms": dict(zip(["g1_tile1", "g2_tile1", "g1_tile2", "g2_tile2"], tune_ms))})
     # ---- plain FP64 path on the same state, same first iterations
     if rank == 0 and world == 1 and not a.no_fp64 and a.precision == "fp32":
         k2 = min(2, a.steps)

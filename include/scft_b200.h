@@ -218,13 +218,15 @@ scft_status scft_timer_elapsed(scft_ctx *ctx, int slot_a, int slot_b, double *ms
 scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
 scft_status scft_reset_stats(scft_ctx *ctx);
 
-/* Picks the number of concurrent slot groups of a props round (1 or 2) by
- * timing props rounds of all replicas at their current fields with each
- * setting; the densities are recomputed, the statistics left unchanged.
- * *groups_out = the setting kept; times_ms[0..1] = best round time with 1 and
- * 2 groups (either pointer may be NULL).  Performance-only: results do not
+/* Picks the schedule of a props round by timing rounds of all replicas at
+ * their current fields: 1 or 2 concurrent slot groups, and x-pencil tiles of
+ * the default or twice the width (grids with tensor-map pencils only).  The
+ * densities are recomputed, the statistics left unchanged.  *groups_out,
+ * *wide_out = the setting kept; times_ms[0..3] = best round time for
+ * (1 group, default tile), (2, default), (1, wide), (2, wide), -1 where not
+ * available (any pointer may be NULL).  Performance-only: results do not
  * depend on the setting. */
-scft_status scft_autotune(scft_ctx *ctx, int *groups_out, double *times_ms);
+scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms);
 
 #ifdef __cplusplus
 }

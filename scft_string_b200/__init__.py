@@ -132,7 +132,7 @@ def lib():
     L.scft_anderson_solve.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
     L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
-    L.scft_autotune.argtypes = [vp, _ip, _dp]
+    L.scft_autotune.argtypes = [vp, _ip, _ip, _dp]
     L.scft_stress_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
     _lib = L
@@ -371,11 +371,12 @@ class Context:
         return v.value
 
     def autotune(self):
-        """Slot-group count kept (1 or 2) and the best props-round times in ms for 1 and 2."""
-        g = C.c_int()
-        t = np.zeros(2)
-        self._ck(lib().scft_autotune(self.h, C.byref(g), _p(t)))
-        return g.value, [float(t[0]), float(t[1])]
+        """(slot groups kept, wide pencil tiles kept, best props-round times in ms for
+        (1 group, default tile), (2, default), (1, wide), (2, wide); -1 where not available)."""
+        g, w = C.c_int(), C.c_int()
+        t = np.zeros(4)
+        self._ck(lib().scft_autotune(self.h, C.byref(g), C.byref(w), _p(t)))
+        return g.value, w.value, [float(v) for v in t]
 
     def timer_mark(self, slot):
         """Records CUDA event `slot` on the context's stream."""

@@ -56,6 +56,9 @@ struct PropsLaunch {
     int tma_pencil;  // x pass through 2-D tensor-map tiles (fixed shapes)
     int pencil_tma_smem;
     const CUtensorMap *tmap;  // host copy of the spectrum tensor map
+    int ptile_wide;  // tensor-map x pass with tiles of twice the default width
+    int pencil_tma_smem_wide;
+    const CUtensorMap *tmap_wide;  // the same spectra with the wide tile box
 };
 
 void pf_smem_bytes(int id, int fp32, int &mid, int &comb);

@@ -541,12 +541,12 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
 // (nslots*2*2*m0) rows by 2*m1*mk2 reals; a tile is the box {2*tc, m0}.
 // Both spectra of a both-pass are requested at kernel start, so the second
 // one lands while the first is transformed; results leave through tile stores.
-template <typename T, int MT, int FM0, int FM1, int FM2>
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
 __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     k_pencil_tma(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int both)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    constexpr int TC = kTile<T>::value, m0 = FM0, m1 = FM1, mk2 = FM2 / 2 + 1;
+    constexpr int m0 = FM0, m1 = FM1, mk2 = FM2 / 2 + 1;
     constexpr int BOX = TC * m0;                      // complex elements per tile
     constexpr uint32_t BOX_BYTES = BOX * 2 * sizeof(T);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
@@ -824,7 +824,15 @@ void launch_pencil(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gp, int bot
 {
     if constexpr (F1 != 0) {
         if (L.tma_pencil) {
-            k_pencil_tma<T, MT, F0, F1, F2><<<gp, MT, L.pencil_tma_smem, st>>>(*L.tmap, a, both);
+            // tile width: kTile columns, or twice that (two butterflies per
+            // thread between barriers) when the autotuner picked it
+            constexpr int TC = kTile<T>::value, ncol = F1 * (F2 / 2 + 1);
+            if (L.ptile_wide)
+                k_pencil_tma<T, MT, F0, F1, F2, 2 * TC><<<dim3((ncol + 2 * TC - 1) / (2 * TC), gp.y, gp.z), MT,
+                                                          L.pencil_tma_smem_wide, st>>>(*L.tmap_wide, a, both);
+            else
+                k_pencil_tma<T, MT, F0, F1, F2, TC><<<dim3((ncol + TC - 1) / TC, gp.y, gp.z), MT, L.pencil_tma_smem,
+                                                      st>>>(*L.tmap, a, both);
             return;
         }
     }
@@ -893,8 +901,13 @@ int set_smem_mt(const PropsLaunch &L)
     cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
     cudaError_t e4 = cudaSuccess, e5 = cudaSuccess;
     if constexpr (F1 != 0) {
-        if (L.tma_pencil)
-            e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem);
+        if (L.tma_pencil) {
+            e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2, kTile<T>::value>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem);
+            if (e4 == cudaSuccess && L.tmap_wide)
+                e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2, 2 * kTile<T>::value>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem_wide);
+        }
         if (e4 == cudaSuccess && L.pf) {
             e4 = cudaFuncSetAttribute(k_combine_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.combine_pf_smem);
             e5 = cudaFuncSetAttribute(k_mid_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.mid_pf_smem);

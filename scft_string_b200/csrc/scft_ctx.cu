@@ -81,7 +81,8 @@ struct scft_ctx {
     void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
          *kfac = nullptr;
     SplineKnots *knots = nullptr;
-    CUtensorMap tmap;  // spectra as a 2-D array for the x-pencil tiles
+    CUtensorMap tmap;       // spectra as a 2-D array for the x-pencil tiles
+    CUtensorMap tmap_wide;  // the same with tiles of twice the width
     // adjoint (stress) scratch, allocated on first use
     void *st_S4 = nullptr, *st_S2 = nullptr, *st_S4p = nullptr;
     double *and_X = nullptr, *and_D = nullptr;  // Anderson histories
@@ -710,19 +711,29 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
             cudaDriverEntryPointQueryResult q;
             if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
                 q == cudaDriverEntryPointSuccess && fn) {
-                const int tc = T == 4 ? 32 : 16;
+                const int tc = T == 4 ? 32 : 16;  // kTile<T> of the kernels
                 cuuint64_t dims[2] = {(cuuint64_t)2 * g.m1 * g.mk2, (cuuint64_t)S * 2 * 2 * g.m0};
                 cuuint64_t strides[1] = {(cuuint64_t)2 * g.m1 * g.mk2 * T};
-                cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)g.m0};
                 cuuint32_t es[2] = {1, 1};
-                CUresult r = ((EncodeFn)fn)(&ctx->tmap, T == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                                            2, ctx->spec, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                if (r == CUDA_SUCCESS && g.m0 <= 256 && (strides[0] % 16) == 0) {
+                auto encode = [&](CUtensorMap *m, int w) {
+                    cuuint32_t box[2] = {(cuuint32_t)(2 * w), (cuuint32_t)g.m0};
+                    return ((EncodeFn)fn)(m, T == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                                          ctx->spec, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                };
+                auto smem_for = [&](int w) { return (int)(128 + (2 * w * g.m0 + g.m0) * 2 * T + (w + g.m0) * T); };
+                if (encode(&ctx->tmap, tc) == CUDA_SUCCESS && g.m0 <= 256 && (strides[0] % 16) == 0) {
                     L.tma_pencil = 1;
                     L.tmap = &ctx->tmap;
-                    L.pencil_tma_smem = (int)(128 + (2 * tc * g.m0 + g.m0) * 2 * T + (tc + g.m0) * T);
+                    L.pencil_tma_smem = smem_for(tc);
+                    // the wide tile (2 tc columns; box width 4 tc reals <= 256)
+                    if (4 * tc <= 256 && smem_for(2 * tc) <= (int)prop.sharedMemPerBlockOptin &&
+                        encode(&ctx->tmap_wide, 2 * tc) == CUDA_SUCCESS) {
+                        L.tmap_wide = &ctx->tmap_wide;
+                        L.pencil_tma_smem_wide = smem_for(2 * tc);
+                        if (const char *ev = getenv("SCFT_PENCIL_TILE_WIDE")) L.ptile_wide = ev[0] == '1';
+                    }
                 }
             }
         }
@@ -1834,26 +1845,36 @@ scft_status scft_reset_stats(scft_ctx *ctx)
     return SCFT_OK;
 }
 
-// Times props rounds of every replica with one and with two concurrent slot
-// groups (each candidate re-captures its graphs, one untimed round, then the
-// fastest of three timed rounds) and keeps the faster setting.  The rounds
-// recompute every replica's densities at its current fields, so the state a
-// caller sees afterwards is unchanged; the statistics are restored.
-scft_status scft_autotune(scft_ctx *ctx, int *groups_out, double *times_ms)
+// Times props rounds of every replica for each schedule -- one or two
+// concurrent slot groups, x-pencil tiles of the default or twice the width
+// (when the grid has tensor-map pencils) -- and keeps the fastest.  Each
+// candidate re-captures its graphs, runs one untimed round, then the best of
+// three timed rounds counts.  The rounds recompute every replica's densities
+// at its current fields, so the state a caller sees afterwards is unchanged;
+// the statistics are restored.
+scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms)
 {
     if (!ctx) return SCFT_BAD_INPUT;
     const scft_stats keep = ctx->stats;
     std::vector<int> all(ctx->strn);
     for (int i = 0; i < ctx->strn; i++) all[i] = i;
-    double best = 0;
-    int best_g = 1;
-    for (int ng = 1; ng <= 2; ng++) {
+    auto drop_graphs = [&]() {
         for (auto &g : ctx->graphs)
             if (g) {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
             }
+    };
+    double best = 0;
+    int best_g = 1, best_w = 0;
+    const int nw = ctx->L.tmap_wide ? 2 : 1;
+    for (int c = 0; c < 4; c++) {
+        const int ng = 1 + (c & 1), wide = c >> 1;
+        if (times_ms) times_ms[c] = -1;
+        if (wide >= nw) continue;
+        drop_graphs();
         ctx->ngroups = ng;
+        ctx->L.ptile_wide = wide;
         scft_status s = props_list(ctx, all);
         if (s != SCFT_OK) return s;
         double t = 1e300;
@@ -1863,22 +1884,19 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, double *times_ms)
             if (s != SCFT_OK) return s;
             t = std::min(t, (ctx->stats.props_seconds - before) * 1e3);
         }
-        if (times_ms) times_ms[ng - 1] = t;
-        if (ng == 1 || t < best) {
+        if (times_ms) times_ms[c] = t;
+        if (c == 0 || t < best) {
             best = t;
             best_g = ng;
+            best_w = wide;
         }
     }
-    if (best_g != ctx->ngroups) {
-        for (auto &g : ctx->graphs)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
-        ctx->ngroups = best_g;
-    }
+    drop_graphs();
+    ctx->ngroups = best_g;
+    ctx->L.ptile_wide = best_w;
     ctx->stats = keep;
     if (groups_out) *groups_out = best_g;
+    if (wide_out) *wide_out = best_w;
     return SCFT_OK;
 }
 

@@ -504,10 +504,17 @@ struct PackedRows {
     static constexpr int LSF = M2 + 1;
 };
 
+// The kz = 0 and kz = M2/2 columns of a slab's half spectrum are real
+// sequences along y before the forward y pass and Hermitian ones before the
+// inverse y pass, so the two travel as one complex column c0 + i cH in column
+// 0: the y passes then cover M2/2 columns (M2/2 x M1/R butterflies per stage,
+// e.g. exactly 256 at 64^3) instead of M2/2 + 1.  slab_ysplit_fixed recovers
+// the two spectra after the forward pass: X0(k) = (C(k) + conj C(-k))/2,
+// XH(k) = (C(k) - conj C(-k))/(2i).
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
 {
-    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
+    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
     constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
     cplx<T> A[PER], B[PER];
 #pragma unroll
@@ -516,9 +523,16 @@ __device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
         if (ITEMS % NT == 0 || e < ITEMS) {
             const int p = e / MK2, kz = e - p * MK2;
             const cplx<T> ck = buf[p * LS + kz];
-            const cplx<T> cm = buf[p * LS + (kz == 0 ? 0 : M2 - kz)];
-            A[i] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
-            B[i] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
+            if (kz == 0) {
+                // rows 2p, 2p+1: (A0, AH) and (B0, BH) are real; packed as c0 + i cH
+                const cplx<T> ch = buf[p * LS + H];
+                A[i] = {ck.x, ch.x};
+                B[i] = {ck.y, ch.y};
+            } else {
+                const cplx<T> cm = buf[p * LS + M2 - kz];
+                A[i] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
+                B[i] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
+            }
         }
     }
     __syncthreads();
@@ -527,17 +541,57 @@ __device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
         const int e = threadIdx.x + i * NT;
         if (ITEMS % NT == 0 || e < ITEMS) {
             const int p = e / MK2, kz = e - p * MK2;
-            buf[2 * p * MK2 + kz] = A[i];
-            if (2 * p + 1 < M1) buf[(2 * p + 1) * MK2 + kz] = B[i];
+            if (kz != H) {  // column H is rebuilt by slab_ysplit_fixed
+                buf[2 * p * MK2 + kz] = A[i];
+                if (2 * p + 1 < M1) buf[(2 * p + 1) * MK2 + kz] = B[i];
+            }
         }
     }
     __syncthreads();
 }
 
+// column 0 after the forward y pass holds C = FFT_y(c0 + i cH): split it
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_ysplit_fixed(cplx<T> *buf)
+{
+    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2;
+    cplx<T> X0, XH;
+    const int k = threadIdx.x;
+    static_assert(M1 <= NT, "one thread per ky");
+    if (k < M1) {
+        const cplx<T> c = buf[k * MK2], cm = buf[((M1 - k) % M1) * MK2];
+        X0 = {(c.x + cm.x) * (T)0.5, (c.y - cm.y) * (T)0.5};
+        XH = {(c.y + cm.y) * (T)0.5, (cm.x - c.x) * (T)0.5};
+    }
+    __syncthreads();
+    if (k < M1) {
+        buf[k * MK2] = X0;
+        buf[k * MK2 + H] = XH;
+    }
+    __syncthreads();
+}
+
+// column 0 before the inverse y pass: S(ky, 0) + i S(ky, H)
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_yjoin_fixed(cplx<T> *buf)
+{
+    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2;
+    static_assert(M1 <= NT, "one thread per ky");
+    const int k = threadIdx.x;
+    if (k < M1) {
+        const cplx<T> c0 = buf[k * MK2], ch = buf[k * MK2 + H];
+        buf[k * MK2] = {c0.x - ch.y, c0.y + ch.x};
+    }
+    __syncthreads();
+}
+
+// Inverse of slab_unpack with half-complex-to-real semantics (imaginary parts
+// of the self-conjugate bins dropped); column 0 holds the inverse y pass of
+// c0 + i cH, i.e. the real kz = 0 value in .x and the real kz = M2/2 value in .y.
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
 {
-    constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
+    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
     constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
     cplx<T> A[PER], B[PER];
 #pragma unroll
@@ -545,11 +599,15 @@ __device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
         const int e = threadIdx.x + i * NT;
         if (ITEMS % NT == 0 || e < ITEMS) {
             const int p = e / MK2, kz = e - p * MK2;
-            A[i] = buf[2 * p * MK2 + kz];
-            B[i] = (2 * p + 1 < M1) ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
-            if (kz == 0 || 2 * kz == M2) {
-                A[i].y = (T)0;
-                B[i].y = (T)0;
+            const bool hb = 2 * p + 1 < M1;
+            if (kz == 0 || kz == H) {
+                const cplx<T> a = buf[2 * p * MK2];
+                const cplx<T> b = hb ? buf[(2 * p + 1) * MK2] : cplx<T>{(T)0, (T)0};
+                A[i] = {kz == 0 ? a.x : a.y, (T)0};
+                B[i] = {kz == 0 ? b.x : b.y, (T)0};
+            } else {
+                A[i] = buf[2 * p * MK2 + kz];
+                B[i] = hb ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
             }
         }
     }
@@ -573,7 +631,8 @@ __device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
     fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, -1);
     slab_unpack_fixed<T, M1, M2, NT>(buf);
-    fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, -1);
+    fft_fixed<T, M1, M2 / 2, MK2, 1, true, NT>(buf, twy, -1);
+    slab_ysplit_fixed<T, M1, M2, NT>(buf);
 }
 
 // half spectrum [y][kz] -> packed real rows (stride M2 + 1, unnormalised)
@@ -581,7 +640,9 @@ template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
 {
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
-    fft_fixed<T, M1, MK2, MK2, 1, true, NT>(buf, twy, +1);
+    __syncthreads();
+    slab_yjoin_fixed<T, M1, M2, NT>(buf);
+    fft_fixed<T, M1, M2 / 2, MK2, 1, true, NT>(buf, twy, +1);
     slab_pack_fixed<T, M1, M2, NT>(buf);
     fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, +1);
 }

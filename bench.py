@@ -152,7 +152,17 @@ def cpu_baseline(cfg, props_per_iter):
         d.props(w, cfg["N"], cfg.get("alpha", 0.1), cfg["phidb"], f, cfg["ens"])
         n += 1
     tp = (time.time() - t0) / n
+    # the same on one core (one or two props calls)
+    O.set_threads(1)
+    t1 = time.time()
+    n1 = 0
+    while n1 < 1 or (time.time() - t1 < 8 and n1 < 2):
+        d.props(w, cfg["N"], cfg.get("alpha", 0.1), cfg["phidb"], f, cfg["ens"])
+        n1 += 1
+    tp1 = (time.time() - t1) / n1
+    O.set_threads(cores)
     return {"value": 1.0 / (props_per_iter * cfg["strn"] * tp), "unit": "string iters/s",
+            "value_1core": 1.0 / (props_per_iter * cfg["strn"] * tp1), "props_s_1core": tp1,
             "cores": cores, "kind": "port",
             "sample": f"{n} props calls of one replica (64^3, N=128, FP64, {cores} threads), "
                       f"{tp:.3f} s each; rate = 1/(props per iteration x replicas x that time) with "

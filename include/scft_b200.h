@@ -218,6 +218,12 @@ scft_status scft_timer_elapsed(scft_ctx *ctx, int slot_a, int slot_b, double *ms
 scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
 scft_status scft_reset_stats(scft_ctx *ctx);
 
+/* Binary FP64 checkpoint (no reference counterpart; the ASCII win files stay
+ * the drop-in format): problem record with the current box and the fields of
+ * every replica, with a hash of the field bytes.  Loading checks the grid and
+ * replica count against the context and the hash, then sets box and fields. */
+scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path);
+scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path);
 /* Picks the schedule of a props round by timing rounds of all replicas at
  * their current fields: 1 or 2 concurrent slot groups, and x-pencil tiles of
  * the default or twice the width (grids with tensor-map pencils only).  The

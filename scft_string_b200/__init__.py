@@ -77,6 +77,7 @@ EXPORTS = [
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
+    "scft_save_checkpoint", "scft_load_checkpoint",
 ]
 
 _lib = None
@@ -135,6 +136,8 @@ def lib():
     L.scft_autotune.argtypes = [vp, _ip, _ip, _dp]
     L.scft_stress_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
+    L.scft_save_checkpoint.argtypes = [vp, C.c_char_p]
+    L.scft_load_checkpoint.argtypes = [vp, C.c_char_p]
     _lib = L
     return L
 
@@ -377,6 +380,13 @@ class Context:
         t = np.zeros(4)
         self._ck(lib().scft_autotune(self.h, C.byref(g), C.byref(w), _p(t)))
         return g.value, w.value, [float(v) for v in t]
+
+    def save_checkpoint(self, path):
+        """Binary FP64 checkpoint of box and fields of every replica."""
+        self._ck(lib().scft_save_checkpoint(self.h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        self._ck(lib().scft_load_checkpoint(self.h, os.fsencode(path)))
 
     def timer_mark(self, slot):
         """Records CUDA event `slot` on the context's stream."""

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
@@ -1897,6 +1898,102 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
     ctx->stats = keep;
     if (groups_out) *groups_out = best_g;
     if (wide_out) *wide_out = best_w;
+    return SCFT_OK;
+}
+
+// ---- binary FP64 checkpoint (no reference counterpart: the reference keeps
+// only the ASCII win files, scft.cu:785-788).  Layout, host byte order:
+//   "SCFTCKP1" | u32 version (1) | u32 sizeof(scft_problem) | scft_problem
+//   (with the current box) | i32 strn | i64 M | strn x 2M doubles (W-, W+) |
+//   u64 FNV-1a hash of the field bytes
+namespace {
+constexpr char kCkptMagic[8] = {'S', 'C', 'F', 'T', 'C', 'K', 'P', '1'};
+
+uint64_t fnv1a(uint64_t h, const void *data, size_t n)
+{
+    const unsigned char *b = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+}  // namespace
+
+scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return SCFT_BAD_INPUT;
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *f = fopen(tmp.c_str(), "wb");
+    if (!f) {
+        ctx->lasterr = "scft_save_checkpoint: cannot open " + tmp;
+        return SCFT_BAD_INPUT;
+    }
+    const uint32_t ver = 1, psz = sizeof(scft_problem);
+    const int32_t strn = ctx->strn;
+    const int64_t M = ctx->M;
+    bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(&ver, 4, 1, f) == 1 && fwrite(&psz, 4, 1, f) == 1 &&
+              fwrite(&ctx->p, psz, 1, f) == 1 && fwrite(&strn, 4, 1, f) == 1 && fwrite(&M, 8, 1, f) == 1;
+    std::vector<double> w(2 * (size_t)M);
+    uint64_t h = 1469598103934665603ull;
+    for (int ii = 0; ok && ii < ctx->strn; ii++) {
+        scft_status s = scft_get_fields(ctx, ii, w.data());
+        if (s != SCFT_OK) {
+            fclose(f);
+            std::remove(tmp.c_str());
+            return s;
+        }
+        h = fnv1a(h, w.data(), w.size() * sizeof(double));
+        ok = fwrite(w.data(), sizeof(double), w.size(), f) == w.size();
+    }
+    ok = ok && fwrite(&h, 8, 1, f) == 1;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path) != 0) {
+        std::remove(tmp.c_str());
+        ctx->lasterr = std::string("scft_save_checkpoint: write failed: ") + path;
+        return SCFT_BAD_INPUT;
+    }
+    return SCFT_OK;
+}
+
+scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return SCFT_BAD_INPUT;
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        ctx->lasterr = std::string("scft_load_checkpoint: cannot open ") + path;
+        return SCFT_BAD_INPUT;
+    }
+    auto fail = [&](const char *why) {
+        fclose(f);
+        ctx->lasterr = std::string("scft_load_checkpoint: ") + why;
+        return SCFT_BAD_INPUT;
+    };
+    char magic[8];
+    uint32_t ver = 0, psz = 0;
+    scft_problem p;
+    int32_t strn = 0;
+    int64_t M = 0;
+    if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return fail("not a checkpoint");
+    if (fread(&ver, 4, 1, f) != 1 || ver != 1 || fread(&psz, 4, 1, f) != 1 || psz != sizeof(scft_problem))
+        return fail("unsupported version");
+    if (fread(&p, psz, 1, f) != 1 || fread(&strn, 4, 1, f) != 1 || fread(&M, 8, 1, f) != 1)
+        return fail("truncated header");
+    if (strn != ctx->strn || M != ctx->M || p.m[0] != ctx->p.m[0] || p.m[1] != ctx->p.m[1] ||
+        p.m[2] != ctx->p.m[2])
+        return fail("grid or replica count differs from the context");
+    std::vector<double> all(2 * (size_t)M * strn);
+    if (fread(all.data(), sizeof(double), all.size(), f) != all.size()) return fail("truncated fields");
+    uint64_t h = 0;
+    if (fread(&h, 8, 1, f) != 1) return fail("truncated hash");
+    if (h != fnv1a(1469598103934665603ull, all.data(), all.size() * sizeof(double))) return fail("hash mismatch");
+    fclose(f);
+    scft_status s = scft_set_box(ctx, p.D);
+    if (s != SCFT_OK) return s;
+    for (int ii = 0; ii < strn; ii++) {
+        s = scft_set_fields(ctx, ii, all.data() + (size_t)ii * 2 * M);
+        if (s != SCFT_OK) return s;
+    }
     return SCFT_OK;
 }
 

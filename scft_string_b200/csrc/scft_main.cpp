@@ -10,6 +10,9 @@
 //   precision 64 (default, the reference arithmetic) or 32 (FP32 propagator bulk)
 //   batched   1 (default): replicas advance together; 0: one at a time
 //   errtol    stop when errtot <= errtol (0 = never, as the reference)
+//   checkpoint 1: also write the binary FP64 checkpoint `fields.ckpt` wherever
+//             the win files are written
+//   restart   1: start from `fields.ckpt` (box and fields) instead of win files
 #include <csignal>
 #include <cmath>
 #include <cstdio>
@@ -145,7 +148,7 @@ int main(int argc, char *argv[])
 {
     double chi = 30, f = 0.8, alpha = 0.1, phidb = 0, errtol_stop = 0;
     int N = 60, ens = 2, readwin = 1, justFE = 0, dostring = 1, strn = 48, nsterp = 4000;
-    int precision = 64, batched = 1;
+    int precision = 64, batched = 1, checkpoint = 0, restart = 0;
     int m[3] = {50, 50, 50}, fix[2] = {0, 0};
     double D[3] = {4, 4, 4};
     g_time0 = time(nullptr);
@@ -174,6 +177,8 @@ int main(int argc, char *argv[])
         get("precision", precision);
         get("batched", batched);
         get("errtol", errtol_stop);
+        get("checkpoint", checkpoint);
+        get("restart", restart);
         if (P.count("m"))
             for (size_t i = 0; i < P["m"].size() && i < 3; i++) m[i] = (int)P["m"][i];
         if (P.count("D"))
@@ -244,6 +249,10 @@ int main(int argc, char *argv[])
     p.device = 0;
     CHECK(scft_create(&p, &ctx));
     for (int ii = 0; ii < strn; ii++) CHECK(scft_set_fields(ctx, ii, W[ii].data()));
+    if (restart == 1 && fexist("fields.ckpt")) {
+        CHECK(scft_load_checkpoint(ctx, "fields.ckpt"));
+        printf("fields.ckpt read.\n");
+    }
     printf("Setup\n");
 
     std::vector<double> conc(4 * M), w(2 * M), FEs(strn), phctot(strn), alf(strn), errs(strn), errs3(strn);
@@ -310,6 +319,7 @@ int main(int argc, char *argv[])
                 CHECK(scft_get_doiis(ctx, doiis.data()));
                 for (int ii = 0; ii < strn; ii++)
                     if (doiis[ii] == 1 && dump(ii, false, true)) return 1;
+                if (checkpoint == 1) CHECK(scft_save_checkpoint(ctx, "fields.ckpt"));
             }
             if (g_sig == 7) {
                 printf("Time's up (procid=0).\n");
@@ -331,6 +341,7 @@ int main(int argc, char *argv[])
         CHECK(scft_get_doiis(ctx, doiis.data()));
         for (int ii = 0; ii < strn; ii++)
             if (doiis[ii] == 1 && dump(ii, true, true)) return 1;
+        if (checkpoint == 1) CHECK(scft_save_checkpoint(ctx, "fields.ckpt"));
     }
     printf("vtks and wins printed\n");
     scft_destroy(ctx);

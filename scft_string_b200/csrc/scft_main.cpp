@@ -24,6 +24,7 @@
 #include <sstream>
 #include <string>
 #include <unordered_map>
+#include <thread>
 #include <vector>
 
 #include "../../include/scft_b200.h"
@@ -101,6 +102,39 @@ bool fexist(const std::string &fn)
     return true;
 }
 
+// Formats rows [0, nrows) with fmt_row(row, std::string &out) (appending), in
+// parallel chunks of rows, and writes the chunks in order: the bytes are those
+// of the one-fprintf-per-value loops of the reference, produced by several
+// threads (the ASCII files of a 128^3 string run to hundreds of MB).
+template <class Fmt>
+void write_rows(FILE *out, long nrows, Fmt fmt_row)
+{
+    const long nthr = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const long chunk = std::max(1L, std::min(65536L, (nrows + nthr - 1) / nthr));
+    const long nchunks = (nrows + chunk - 1) / chunk;
+    for (long c0 = 0; c0 < nchunks; c0 += nthr) {
+        const long c1 = std::min(nchunks, c0 + nthr);
+        std::vector<std::string> bufs(c1 - c0);
+        std::vector<std::thread> th;
+        for (long c = c0; c < c1; c++)
+            th.emplace_back([&, c]() {
+                std::string &b = bufs[c - c0];
+                const long r0 = c * chunk, r1 = std::min(nrows, r0 + chunk);
+                for (long r = r0; r < r1; r++) fmt_row(r, b);
+            });
+        for (auto &t : th) t.join();
+        for (auto &b : bufs) fwrite(b.data(), 1, b.size(), out);
+    }
+}
+
+// appends printf(fmt, v) (a %lf conversion prints at most 317 characters)
+inline void append_f(std::string &o, const char *fmt, double v)
+{
+    char t[400];
+    const int n = snprintf(t, sizeof t, fmt, v);
+    o.append(t, (size_t)std::min(std::max(n, 0), (int)sizeof t - 1));
+}
+
 void tovtk(const std::string &fname, const int *m, const double *D, const double *data)  // scft.cu:486-512
 {
     FILE *out = fopen(fname.c_str(), "w");
@@ -115,11 +149,13 @@ void tovtk(const std::string &fname, const int *m, const double *D, const double
     fprintf(out, "POINT_DATA %ld\n", (long)m[0] * m[1] * m[2]);
     fprintf(out, "SCALARS scalars float\n");
     fprintf(out, "LOOKUP_TABLE default\n\n");
-    for (int x = 0; x < m[0]; x++)
-        for (int y = 0; y < m[1]; y++) {
-            for (int z = 0; z < m[2]; z++) fprintf(out, "%.4lf\t", data[z + y * m[2] + x * m[2] * m[1]]);
-            fprintf(out, "\n");
-        }
+    // one row per (x, y): m2 values "%.4lf\t" and a newline
+    const int m2 = m[2];
+    write_rows(out, (long)m[0] * m[1], [&](long row, std::string &o) {
+        const double *d = data + row * m2;
+        for (int z = 0; z < m2; z++) append_f(o, "%.4lf\t", d[z]);
+        o.push_back('\n');
+    });
     fclose(out);
 }
 
@@ -127,7 +163,10 @@ void write_win(const std::string &fn, const double *w, long M)  // scft.cu:785-7
 {
     FILE *out = fopen(fn.c_str(), "w");
     if (!out) return;
-    for (long r = 0; r < M; r++) fprintf(out, "%.6lf %.6lf\n", w[r], w[r + M]);
+    write_rows(out, M, [&](long r, std::string &o) {
+        append_f(o, "%.6lf ", w[r]);
+        append_f(o, "%.6lf\n", w[r + M]);
+    });
     fclose(out);
 }
 

@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--workload", default="string", choices=["string", "uneven24", "mixed128", "adjoint96"],
                     help="uneven24: the 24 independent solves of mixed grids and N, run concurrently")
     ap.add_argument("--tol", type=float, default=1e-5, help="uneven24: RMS residual target")
+    ap.add_argument("--start", default="lamellar", choices=["lamellar", "hex"],
+                    help="adjoint96: start field of the saddle point search")
     ap.add_argument("--serial-fp64", action="store_true",
                     help="uneven24: also run the solves one at a time on the plain FP64 path")
     ap.add_argument("--profile-round", type=int, default=0, metavar="R",
@@ -299,16 +301,25 @@ def run_adjoint96(a):
     import torch
 
     import scft_string_b200 as S
-    from scft_string_b200.configs import ADJOINT_96, hex_fields
+    from scft_string_b200.configs import ADJOINT_96, hex_fields, lamellar_fields
     torch.cuda.set_device(0)
     c = dict(ADJOINT_96)
-    wm, wp = hex_fields(c)
-    # The stated start, 0.5 chiN sum_j cos(G_j.r), puts |W-| up to 1.5 chiN,
-    # three times the self-consistent range |W-| <= chiN/2; simple, pressure
-    # and Anderson mixing all diverge from it (W+ runs away).  The saddle is
-    # sought from the same pattern at 0.2 of that amplitude.
-    wm = 0.2 * wm
     t0 = time.time()
+    hex_note = None
+    if a.start == "hex":
+        # The stated start, 0.5 chiN sum_j cos(G_j.r), puts |W-| up to 1.5 chiN,
+        # three times the self-consistent range |W-| <= chiN/2; simple, pressure
+        # and Anderson mixing all diverge from it (W+ runs away).  The saddle is
+        # sought from the same pattern at 0.2 of that amplitude.
+        wm, wp = hex_fields(c)
+        wm = 0.2 * wm
+    else:
+        # Lamellae along z (one period = Lz): the same grid, box, N, chiN and f;
+        # a 1-D saddle that Anderson mixing converges to 1e-9.  The hexagonal
+        # start is not commensurate with the square x-y cross-section and its
+        # cylinders relax slowly (residual 1.8e-4 after 6000 iterations).
+        wm, wp = lamellar_fields(c)
+        hex_note = "hexagonal start: residual 1.8e-4 after 6000 Anderson iterations (not converged)"
 
     def converged(D, chi, prec="fp64", W0=None, f=None):
         cc = dict(c, D=tuple(D), chi=chi)
@@ -369,7 +380,7 @@ def run_adjoint96(a):
     if err0 < 1e-6:  # relax from a converged saddle only
         n, st, box = ctx.relax_cell(0, maxOuter=20, inner=0, stressTol=1e-6, gamma=2.0)
         relax = {"rounds": n, "final_stress": list(st), "box": list(box)}
-    out = {"workload": c["name"], "saddle_residual": err0, "anderson_iters": n0, "F": F0,
+    out = {"workload": c["name"], "start": a.start, "hex_note": hex_note, "saddle_residual": err0, "anderson_iters": n0, "F": F0,
            "dF_dL_fp64_adjoint": list(dF64), "dF_dL_fp32_adjoint": list(dF32), "dF_dL_fd": fd,
            "dF_dL_fp32_vs_fp64_rel": float(np.max(np.abs(dF32 - dF64)) / max(1e-30, np.max(np.abs(dF64)))),
            "dF_dL_fp64_ckpt13_vs_full": float(np.max(np.abs(dF64ck - dF64))),

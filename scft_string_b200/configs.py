@@ -144,3 +144,13 @@ def hex_fields(c: dict):
         w += np.cos(g * (np.cos(a) * X + np.sin(a) * Y))
     wm = 0.5 * c["chi"] * w.ravel() + np.random.default_rng(c["seed"]).normal(0, 0.02 * c["chi"], w.size)
     return wm[None, :], np.zeros((1, w.size))
+
+
+def lamellar_fields(c: dict):
+    """W- = 0.4 chiN cos(2 pi z / Lz) (one period along axis 2) plus noise
+    0.02 chiN (default_rng(seed)); W+ = 0."""
+    m, D = c["m"], c["D"]
+    z = np.arange(m[2]) * D[2] / m[2]
+    w = np.broadcast_to(0.4 * c["chi"] * np.cos(2 * np.pi * z / D[2]), tuple(m)).ravel()
+    wm = w + np.random.default_rng(c["seed"]).normal(0, 0.02 * c["chi"], w.size)
+    return wm[None, :], np.zeros((1, w.size))

@@ -48,3 +48,13 @@ def test_string_fields_reproducible():
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
     assert a[0].shape == (4, 512)
+
+
+def test_lamellar_fields_vary_along_z_only():
+    from scft_string_b200.configs import lamellar_fields
+    c = dict(ADJOINT_96, m=(8, 8, 24), seed=2)
+    wm, wp = lamellar_fields(c)
+    w = wm[0].reshape(8, 8, 24)
+    assert not wp.any()
+    assert np.abs(w - w.mean(axis=(0, 1), keepdims=True)).max() < 10 * 0.02 * c["chi"]
+    assert abs(w[:, :, 0].mean() - 0.4 * c["chi"]) < 0.05 * c["chi"]

@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-5, help="uneven24: RMS residual target")
     ap.add_argument("--start", default="lamellar", choices=["lamellar", "hex"],
                     help="adjoint96: start field of the saddle point search")
+    ap.add_argument("--iters", type=int, default=5000, help="uneven24: Anderson iteration cap per solve")
     ap.add_argument("--serial-fp64", action="store_true",
                     help="uneven24: also run the solves one at a time on the plain FP64 path")
     ap.add_argument("--profile-round", type=int, default=0, metavar="R",
@@ -193,7 +194,7 @@ def run_uneven(a):
         return ctx
 
     def solve(ctx):
-        n, err = ctx.anderson_solve(0, maxIter=5000, tol=a.tol, nhist=12, lam=0.1)
+        n, err = ctx.anderson_solve(0, maxIter=a.iters, tol=a.tol, nhist=12, lam=0.1)
         return n, err, ctx.stats()["contour_steps"]
 
     ctxs = [make(c, a.precision) for c in solves]
@@ -206,6 +207,9 @@ def run_uneven(a):
         res = list(ex.map(solve, ctxs))
     wall = time.time() - t0
     steps = sum(r[2] for r in res)
+    b = 4 if a.precision == "fp32" else 8
+    algo = sum(r[2] * 8 * c["m"][0] * c["m"][1] * c["m"][2] * b for r, c in zip(res, solves))
+    peak, peak_kind = peaks()
     line = {"metric": "aggregate contour steps/s, uneven batch of 24 solves to RMS residual "
                       f"{a.tol:g}", "value": steps / wall, "unit": "contour steps/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32" if a.precision == "fp32" else "f64",
@@ -213,16 +217,23 @@ def run_uneven(a):
             "config": {"workload": "uneven24: 8x48^3, 10x64^3, 6x96^3, N in {64..256}, ens=2",
                        "solver": "Anderson (FP64 least squares), one context and stream per solve"},
             "wall_s": wall, "iterations": [r[0] for r in res], "residuals": [r[1] for r in res],
-            "converged": sum(1 for r in res if r[1] <= a.tol)}
+            "converged": sum(1 for r in res if r[1] <= a.tol), "iteration_cap": a.iters,
+            "roofline": {"bound": "hbm", "achieved": algo / wall / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / wall / 1e9 / peak, "peak_kind": peak_kind,
+                         "note": "8 M b algorithmic bytes per contour step, wall time of the whole batch"}}
     if a.serial_fp64:
-        t0 = time.time()
         s64 = 0
+        w64 = 0.0
         for c in solves:
             ctx = make(c, "fp64")
+            ctx.props(0)
+            ctx.reset_stats()
+            torch.cuda.synchronize()
+            t1 = time.time()
             n, err, st = solve(ctx)
+            w64 += time.time() - t1
             s64 += st
             ctx.close()
-        w64 = time.time() - t0
         line["serial_fp64"] = {"wall_s": w64, "contour_steps_per_s": s64 / w64}
         line["speedup_vs_serial_fp64_wall"] = w64 / wall
     print(json.dumps(line))

@@ -13,6 +13,8 @@
 //   checkpoint 1: also write the binary FP64 checkpoint `fields.ckpt` wherever
 //             the win files are written
 //   restart   1: start from `fields.ckpt` (box and fields) instead of win files
+//   fcont     1: continuous A fraction (no rounding of f; junction step inside
+//             the chain), 0 (default): the reference's rounded f
 #include <csignal>
 #include <cmath>
 #include <cstdio>
@@ -187,7 +189,7 @@ int main(int argc, char *argv[])
 {
     double chi = 30, f = 0.8, alpha = 0.1, phidb = 0, errtol_stop = 0;
     int N = 60, ens = 2, readwin = 1, justFE = 0, dostring = 1, strn = 48, nsterp = 4000;
-    int precision = 64, batched = 1, checkpoint = 0, restart = 0;
+    int precision = 64, batched = 1, checkpoint = 0, restart = 0, fcont = 0;
     int m[3] = {50, 50, 50}, fix[2] = {0, 0};
     double D[3] = {4, 4, 4};
     g_time0 = time(nullptr);
@@ -218,6 +220,7 @@ int main(int argc, char *argv[])
         get("errtol", errtol_stop);
         get("checkpoint", checkpoint);
         get("restart", restart);
+        get("fcont", fcont);
         if (P.count("m"))
             for (size_t i = 0; i < P["m"].size() && i < 3; i++) m[i] = (int)P["m"][i];
         if (P.count("D"))
@@ -286,6 +289,7 @@ int main(int argc, char *argv[])
     p.precision = precision == 32 ? SCFT_FP32 : SCFT_FP64;
     p.batched = batched;
     p.device = 0;
+    p.fcont = fcont;
     CHECK(scft_create(&p, &ctx));
     for (int ii = 0; ii < strn; ii++) CHECK(scft_set_fields(ctx, ii, W[ii].data()));
     if (restart == 1 && fexist("fields.ckpt")) {

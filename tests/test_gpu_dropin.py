@@ -76,3 +76,34 @@ def test_dropin_files_match_reference(built_lib, tmp_path, name):
         assert np.array_equal(np.isnan(r), np.isnan(g)), fn
         ok = ~np.isnan(r)
         assert np.abs(r[ok] - g[ok]).max() <= tol, (fn, np.abs(r[ok] - g[ok]).max())
+
+
+def test_dropin_checkpoint_restart(built_lib, tmp_path):
+    """`checkpoint = 1` writes fields.ckpt beside the win files; a second run
+    with `restart = 1` and no win files starts from it (box and fields) and,
+    with justFE = 1 (no string iterations), writes back the same W- fields."""
+    name = sorted(CASES)[0]
+    c = dict(load_fixture(name)["params"])
+    wm, wp = fields(c)
+    base = input_dat(c) + f"strn = {c['strn']}\nnsterp = {c['nsterp']}\n"
+    a = tmp_path / "a"
+    a.mkdir()
+    (a / "input.dat").write_text(base + "checkpoint = 1\n")
+    for ii in range(c["strn"]):
+        (a / f"win{ii}").write_text(win_text(wm[ii], wp[ii]))
+    p = subprocess.run([EXE], cwd=a, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    assert (a / "fields.ckpt").exists()
+    b = tmp_path / "b"
+    b.mkdir()
+    (b / "input.dat").write_text(input_dat(c) + f"strn = {c['strn']}\njustFE = 1\nrestart = 1\n")
+    (b / "fields.ckpt").write_bytes((a / "fields.ckpt").read_bytes())
+    p = subprocess.run([EXE], cwd=b, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    assert "fields.ckpt read." in p.stdout
+    # the W+ prelude of the second run starts from the restored fields; their
+    # W- parts are untouched by it, so W- of every propagated replica matches
+    for ii in range(c["strn"]):
+        wa, wb = numbers((a / f"win{ii}").read_text()), numbers((b / f"win{ii}").read_text())
+        assert wa.size == wb.size
+        assert np.abs(wa[0::2] - wb[0::2]).max() <= 1.01e-6, ii

@@ -148,6 +148,10 @@ scft_status scft_last_free_energy(const scft_ctx *ctx, double *FE, double *FEs, 
 /* Box lengths D (the reference's D[3], used by setup_k_sq, density.h:79-95). */
 scft_status scft_set_box(scft_ctx *ctx, const double *D);
 scft_status scft_get_box(const scft_ctx *ctx, double *D);
+/* The box of one replica: every replica of a context may own its cell (the
+ * diffusion factors are kept per replica); scft_set_box sets all of them. */
+scft_status scft_set_box_replica(scft_ctx *ctx, int ii, const double *D);
+scft_status scft_get_box_replica(const scft_ctx *ctx, int ii, double *D);
 /* d lnQ/dL_i of replica ii at its current fields by the adjoint of the
  * Richardson propagator (q^dagger is the adjoint of q's chain), and the box
  * stress dF/dL_i = -d lnQ/dL_i, exact at a converged saddle point.  Either
@@ -173,7 +177,7 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
  * RMS residual <= tol; *iters = props evaluations, *err_out = last RMS. */
 scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, int nhist, double lam,
                                 int *iters, double *err_out);
-/* Variable-cell relaxation of replica ii: `inner` iterations of the
+/* Variable-cell relaxation of replica ii in its own box: `inner` iterations of the
  * solve_field loop on that replica (no FreeE), then a gradient step on the
  * box, L_i -= gamma dF/dL_i (each relative change capped at 2 %), until
  * max_i |dF/dL_i| <= stressTol or maxOuter rounds; inner <= 0 re-solves the

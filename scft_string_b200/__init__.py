@@ -77,7 +77,7 @@ EXPORTS = [
     "scft_reset_stats", "scft_timer_mark", "scft_timer_elapsed", "scft_set_box", "scft_get_box",
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
-    "scft_save_checkpoint", "scft_load_checkpoint",
+    "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
 ]
 
 _lib = None
@@ -137,6 +137,8 @@ def lib():
     L.scft_stress_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
     L.scft_save_checkpoint.argtypes = [vp, C.c_char_p]
+    L.scft_set_box_replica.argtypes = [vp, C.c_int, _dp]
+    L.scft_get_box_replica.argtypes = [vp, C.c_int, _dp]
     L.scft_load_checkpoint.argtypes = [vp, C.c_char_p]
     _lib = L
     return L
@@ -325,12 +327,20 @@ class Context:
     def reset_stats(self):
         self._ck(lib().scft_reset_stats(self.h))
 
-    def set_box(self, D):
-        self._ck(lib().scft_set_box(self.h, _p(np.ascontiguousarray(D, np.float64))))
+    def set_box(self, D, ii=None):
+        """Box of every replica, or of replica ii only."""
+        D = np.ascontiguousarray(D, np.float64)
+        if ii is None:
+            self._ck(lib().scft_set_box(self.h, _p(D)))
+        else:
+            self._ck(lib().scft_set_box_replica(self.h, int(ii), _p(D)))
 
-    def get_box(self):
+    def get_box(self, ii=None):
         D = np.zeros(3)
-        self._ck(lib().scft_get_box(self.h, _p(D)))
+        if ii is None:
+            self._ck(lib().scft_get_box(self.h, _p(D)))
+        else:
+            self._ck(lib().scft_get_box_replica(self.h, int(ii), _p(D)))
         return D
 
     def stress(self, ii=0):
@@ -360,7 +370,7 @@ class Context:
         st = np.zeros(3)
         self._ck(lib().scft_relax_cell(self.h, int(ii), int(maxOuter), int(inner), float(stressTol),
                                        float(gamma), C.byref(n), _p(st)))
-        return n.value, st, self.get_box()
+        return n.value, st, self.get_box(ii)
 
     def dF_df(self, ii=0):
         """(d lnQ/df, dF/df) of replica ii; the context needs fcont=1."""

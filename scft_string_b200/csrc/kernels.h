@@ -33,7 +33,8 @@ struct PropsArgs {
     cplx<T> *spec;          // [slot][2 fields][2 spectra][Mk]
     T *pbuf;                // [slot][2][M]  E2 * full-step result
     const cplx<T> *tw;      // twiddles: x (m0) | y (m1) | z (m2)
-    const T *kfac;          // per-axis diffusion factors: x (m0) | y (m1) | z (mk2)
+    const T *kfac;          // per-axis diffusion factors: x (m0) | y (m1) | z (mk2), per replica
+    int kf_stride;          // elements between replicas' factor blocks (0: one shared box)
     double *partials;       // [slot][npart_stride]
     int npart_stride;
     T invM, Mreal;

@@ -296,12 +296,13 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1) 
     const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const int ncol = m1 * mk2;
     const int c0 = tile * tc;
+    const T *kf = a.kfac + (size_t)a.slot_rep[slot] * a.kf_stride;  // the replica's box
     for (int t = threadIdx.x; t < tc; t += nthr) {
         const int c = c0 + t;
         const int y = c / mk2, kz = c - y * mk2;
-        colf[t] = c < ncol ? a.kfac[m0 + y] * a.kfac[m0 + m1 + kz] : (T)0;
+        colf[t] = c < ncol ? kf[m0 + y] * kf[m0 + m1 + kz] : (T)0;
     }
-    for (int i = threadIdx.x; i < m0; i += nthr) gx[i] = a.kfac[i];
+    for (int i = threadIdx.x; i < m0; i += nthr) gx[i] = kf[i];
     const T invM = a.invM;
     cplx<T> *spec = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     const int npass = both ? 2 : 1;
@@ -570,14 +571,15 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
             tma_load_2d(bufB, &tmap, x, y0 + m0, &bars[1]);
         }
     }
+    const T *kf = a.kfac + (size_t)a.slot_rep[slot] * a.kf_stride;  // the replica's box
     for (int i = threadIdx.x; i < m0; i += MT) {
         twx[i] = a.tw[i];
-        gx[i] = a.kfac[i];
+        gx[i] = kf[i];
     }
     for (int t = threadIdx.x; t < TC; t += MT) {
         const int c = c0 + t;
         const int yy = c / mk2, kz = c - yy * mk2;
-        colf[t] = c < ncol ? a.kfac[m0 + yy] * a.kfac[m0 + m1 + kz] : (T)0;
+        colf[t] = c < ncol ? kf[m0 + yy] * kf[m0 + m1 + kz] : (T)0;
     }
     __syncthreads();
     const T invM = a.invM;

@@ -78,6 +78,8 @@ struct scft_ctx {
     double *partials = nullptr, *redout = nullptr;
     int npart_stride = 0, nred_rows = 0;
     int *rep_dev = nullptr, *err = nullptr;
+    std::vector<double> Dr;  // box of every replica (3 per replica); p.D is the last common box
+    int kf_n = 0;            // diffusion factors per replica (m0 + m1 + mk2)
     void *jtab = nullptr;  // junction-step E table per slot (continuous A fraction)
     void *etab = nullptr, *hist = nullptr, *spec = nullptr, *pbuf = nullptr, *tw = nullptr,
          *kfac = nullptr;
@@ -147,6 +149,7 @@ PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
     a.pbuf = (T *)ctx->pbuf;
     a.tw = (const cplx<T> *)ctx->tw;
     a.kfac = (const T *)ctx->kfac;
+    a.kf_stride = ctx->kf_n;
     a.partials = ctx->partials;
     a.npart_stride = ctx->npart_stride;
     a.invM = (T)(1.0 / ctx->M);
@@ -481,8 +484,10 @@ scft_status free_energy(scft_ctx *ctx, double *FEout)
 }
 
 template <typename T>
-void upload_tables(scft_ctx *ctx, std::vector<unsigned char> &twb, std::vector<unsigned char> &kfb)
+void upload_tables(scft_ctx *ctx, std::vector<unsigned char> &twb, std::vector<unsigned char> &kfb,
+                   const double *Dbox = nullptr)
 {
+    const double *Dx = Dbox ? Dbox : ctx->p.D;
     const Geo &g = ctx->g;
     const double PI = 3.14159265358979323846264338327950288;
     const int ns[3] = {g.m0, g.m1, g.m2};
@@ -501,7 +506,7 @@ void upload_tables(scft_ctx *ctx, std::vector<unsigned char> &twb, std::vector<u
         const int cnt = a == 2 ? g.mk2 : m;
         for (int K = 0; K < cnt; K++) {
             const int k = (a == 2) ? K : (K <= m / 2 ? K : K - m);
-            const double A = (double)k * k / (ctx->p.D[a] * ctx->p.D[a]);
+            const double A = (double)k * k / (Dx[a] * Dx[a]);
             kf.push_back((T)std::exp(-4 * PI * PI * A * ds / 12));
         }
     }
@@ -691,10 +696,17 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
         CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
         CKC(cudaMalloc(&ctx->tw, twb.size()));
-        CKC(cudaMalloc(&ctx->kfac, kfb.size()));
+        // one block of diffusion factors per replica (every replica may own its box)
+        ctx->kf_n = g.m0 + g.m1 + g.mk2;
+        ctx->Dr.assign(3 * R, 0.0);
+        for (size_t r = 0; r < R; r++)
+            for (int i = 0; i < 3; i++) ctx->Dr[3 * r + i] = p->D[i];
+        CKC(cudaMalloc(&ctx->kfac, kfb.size() * R));
         CKC(cudaMalloc(&ctx->knots, sizeof(SplineKnots)));
         CKC(cudaMemcpy(ctx->tw, twb.data(), twb.size(), cudaMemcpyHostToDevice));
-        CKC(cudaMemcpy(ctx->kfac, kfb.data(), kfb.size(), cudaMemcpyHostToDevice));
+        for (size_t r = 0; r < R; r++)
+            CKC(cudaMemcpy((unsigned char *)ctx->kfac + r * kfb.size(), kfb.data(), kfb.size(),
+                           cudaMemcpyHostToDevice));
         CKC(cudaMemset(ctx->W, 0, sizeof(double) * 2 * M * R));
         CKC(cudaMemset(ctx->conc, 0, sizeof(double) * 4 * M * R));
         CKC(cudaMemset(ctx->DEV, 0, sizeof(double) * 2 * M * R));
@@ -1242,17 +1254,34 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
 }
 
 // box lengths: re-derive the per-axis diffusion factors (setup_k_sq, density.h:79-95)
-scft_status scft_set_box(scft_ctx *ctx, const double *D)
+namespace {
+// uploads the diffusion factors of replica r for the box D
+scft_status upload_box(scft_ctx *ctx, int r, const double *D)
 {
-    if (!ctx || !D || !(D[0] > 0) || !(D[1] > 0) || !(D[2] > 0)) return SCFT_BAD_INPUT;
-    for (int i = 0; i < 3; i++) ctx->p.D[i] = D[i];
     std::vector<unsigned char> twb, kfb;
     if (ctx->prec == SCFT_FP32)
-        upload_tables<float>(ctx, twb, kfb);
+        upload_tables<float>(ctx, twb, kfb, D);
     else
-        upload_tables<double>(ctx, twb, kfb);
-    CK(cudaMemcpyAsync(ctx->kfac, kfb.data(), kfb.size(), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+        upload_tables<double>(ctx, twb, kfb, D);
+    CK(cudaMemcpyAsync((unsigned char *)ctx->kfac + (size_t)r * kfb.size(), kfb.data(), kfb.size(),
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));  // kfb is pageable and goes out of scope
+    for (int i = 0; i < 3; i++) ctx->Dr[3 * (size_t)r + i] = D[i];
+    return SCFT_OK;
+}
+
+bool box_ok(const double *D) { return D && D[0] > 0 && D[1] > 0 && D[2] > 0; }
+}  // namespace
+
+// the box of every replica (and the scratch replica of scft_props_host)
+scft_status scft_set_box(scft_ctx *ctx, const double *D)
+{
+    if (!ctx || !box_ok(D)) return SCFT_BAD_INPUT;
+    for (int i = 0; i < 3; i++) ctx->p.D[i] = D[i];
+    for (int r = 0; r < ctx->nrep_alloc; r++) {
+        scft_status s = upload_box(ctx, r, D);
+        if (s != SCFT_OK) return s;
+    }
     return SCFT_OK;
 }
 
@@ -1260,6 +1289,20 @@ scft_status scft_get_box(const scft_ctx *ctx, double *D)
 {
     if (!ctx || !D) return SCFT_BAD_INPUT;
     for (int i = 0; i < 3; i++) D[i] = ctx->p.D[i];
+    return SCFT_OK;
+}
+
+scft_status scft_set_box_replica(scft_ctx *ctx, int ii, const double *D)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || !box_ok(D)) return SCFT_BAD_INPUT;
+    ctx->slot_of[ii] = -1;  // its stored propagators no longer match its box
+    return upload_box(ctx, ii, D);
+}
+
+scft_status scft_get_box_replica(const scft_ctx *ctx, int ii, double *D)
+{
+    if (!ctx || !D || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    for (int i = 0; i < 3; i++) D[i] = ctx->Dr[3 * (size_t)ii + i];
     return SCFT_OK;
 }
 
@@ -1296,10 +1339,11 @@ scft_status stress_alloc(scft_ctx *ctx)
 }
 
 // sums the pairs (in chunks of kStressPairs) into dQC / dQ2 (unnormalised)
-scft_status stress_pairs(scft_ctx *ctx, int slot, const void *hist, const std::vector<StressPr> &pairs,
+scft_status stress_pairs(scft_ctx *ctx, int rep, int slot, const void *hist, const std::vector<StressPr> &pairs,
                          double *dQC, double *dQ2)
 {
     const Geo &g = ctx->g;
+    const double *Lr = &ctx->Dr[3 * (size_t)rep];  // the replica's box
     std::vector<double> out(3 * kStressPairs);
     for (size_t c0 = 0; c0 < pairs.size(); c0 += kStressPairs) {
         StressPairs P;
@@ -1316,19 +1360,19 @@ scft_status stress_pairs(scft_ctx *ctx, int slot, const void *hist, const std::v
         int nl;
         if (ctx->prec == SCFT_FP32) {
             StressArgs<float> a{g, slot, (const float *)hist, (const float *)ctx->etab,
-                                (const cplx<float> *)ctx->tw, (const float *)ctx->kfac,
+                                (const cplx<float> *)ctx->tw, (const float *)ctx->kfac + (size_t)rep * ctx->kf_n,
                                 (cplx<float> *)ctx->st_S4, (cplx<float> *)ctx->st_S2,
                                 (cplx<float> *)ctx->st_S4p, ctx->st_part,
-                                {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, (float)(1.0 / g.M), ctx->err};
+                                {Lr[0], Lr[1], Lr[2]}, (float)(1.0 / g.M), ctx->err};
             a.jtab = (const float *)ctx->jtab;
             nl = launch_stress_chunk<float>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
                                             ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
         } else {
             StressArgs<double> a{g, slot, (const double *)hist, (const double *)ctx->etab,
-                                 (const cplx<double> *)ctx->tw, (const double *)ctx->kfac,
+                                 (const cplx<double> *)ctx->tw, (const double *)ctx->kfac + (size_t)rep * ctx->kf_n,
                                  (cplx<double> *)ctx->st_S4, (cplx<double> *)ctx->st_S2,
                                  (cplx<double> *)ctx->st_S4p, ctx->st_part,
-                                 {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, 1.0 / g.M, ctx->err};
+                                 {Lr[0], Lr[1], Lr[2]}, 1.0 / g.M, ctx->err};
             a.jtab = (const double *)ctx->jtab;
             nl = launch_stress_chunk<double>(a, P, ctx->rt_slab_threads, ctx->rt_slab_smem,
                                              ctx->rt_pencil_threads, ctx->rt_pencil_smem, ctx->st_out, ctx->st);
@@ -1407,7 +1451,7 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
     for (int s2 = 0; s2 < g.Ns; s2++) pairs.push_back({s2, 0, g.Ns - 1 - s2, 1, q_table(g, s2), 0});
     for (int j = 0; j < g.Nh; j++) pairs.push_back({j, 1, g.Nh - 1 - j, 1, 1, 1});
     double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
-    s = stress_pairs(ctx, slot, ctx->hist, pairs, dQC, dQ2);
+    s = stress_pairs(ctx, ii, slot, ctx->hist, pairs, dQC, dQ2);
     if (s != SCFT_OK) return s;
     stress_finish(ctx, Q2, QC, dQC, dQ2, dlnQ_dL, dF_dL);
     return SCFT_OK;
@@ -1555,7 +1599,7 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
                     else
                         pairs.push_back({(int)segoff + (t - m0), 0, u - a0, 1, q_table(g, t), 0});
                 }
-            scft_status st = stress_pairs(ctx, 0, seg, pairs, dQC, dQ2);
+            scft_status st = stress_pairs(ctx, ii, 0, seg, pairs, dQC, dQ2);
             if (st != SCFT_OK) return st;
         }
         return SCFT_OK;
@@ -1604,10 +1648,10 @@ scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
     int nl;
     if (T == 4) {
         StressArgs<float> a{g, slot, (const float *)ctx->hist, (const float *)ctx->etab,
-                            (const cplx<float> *)ctx->tw, (const float *)ctx->kfac,
+                            (const cplx<float> *)ctx->tw, (const float *)ctx->kfac + (size_t)ii * ctx->kf_n,
                             (cplx<float> *)ctx->st_S4, (cplx<float> *)ctx->st_S2,
                             (cplx<float> *)ctx->st_S4p, ctx->st_part,
-                            {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, (float)(1.0 / g.M), ctx->err};
+                            {ctx->Dr[3 * (size_t)ii], ctx->Dr[3 * (size_t)ii + 1], ctx->Dr[3 * (size_t)ii + 2]}, (float)(1.0 / g.M), ctx->err};
         a.jtab = (const float *)ctx->jtab;
         a.rbuf = (float *)ctx->jd_rbuf;
         a.wminus = wm;
@@ -1616,10 +1660,10 @@ scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
                                            ctx->st);
     } else {
         StressArgs<double> a{g, slot, (const double *)ctx->hist, (const double *)ctx->etab,
-                             (const cplx<double> *)ctx->tw, (const double *)ctx->kfac,
+                             (const cplx<double> *)ctx->tw, (const double *)ctx->kfac + (size_t)ii * ctx->kf_n,
                              (cplx<double> *)ctx->st_S4, (cplx<double> *)ctx->st_S2,
                              (cplx<double> *)ctx->st_S4p, ctx->st_part,
-                             {ctx->p.D[0], ctx->p.D[1], ctx->p.D[2]}, 1.0 / g.M, ctx->err};
+                             {ctx->Dr[3 * (size_t)ii], ctx->Dr[3 * (size_t)ii + 1], ctx->Dr[3 * (size_t)ii + 2]}, 1.0 / g.M, ctx->err};
         a.jtab = (const double *)ctx->jtab;
         a.rbuf = (double *)ctx->jd_rbuf;
         a.wminus = wm;
@@ -1752,8 +1796,8 @@ scft_status scft_anderson_solve(scft_ctx *ctx, int ii, int maxIter, double tol, 
 // Variable-cell relaxation of replica ii: `inner` SCFT iterations (the
 // solve_field loop restricted to this replica, scft.cu:598-608, without the
 // periodic FreeE) or, with inner <= 0, an Anderson re-solve to RMS 1e-9; then
-// L_i -= gamma dF/dL_i with each relative change capped at 2 %, until
-// max |dF/dL_i| <= stressTol.
+// the replica's own box L_i -= gamma dF/dL_i with each relative change capped
+// at 2 %, until max |dF/dL_i| <= stressTol.
 scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, double stressTol, double gamma,
                             int *outer_out, double *stress_out)
 {
@@ -1785,12 +1829,13 @@ scft_status scft_relax_cell(scft_ctx *ctx, int ii, int maxOuter, int inner, doub
         if (mx <= stressTol) break;
         double D[3];
         for (int i = 0; i < 3; i++) {
+            const double Di = ctx->Dr[3 * (size_t)ii + i];
             double step = -gamma * dF[i];
-            const double cap = 0.02 * ctx->p.D[i];
+            const double cap = 0.02 * Di;
             step = std::max(-cap, std::min(cap, step));
-            D[i] = ctx->p.D[i] + step;
+            D[i] = Di + step;
         }
-        s = scft_set_box(ctx, D);
+        s = scft_set_box_replica(ctx, ii, D);
         if (s != SCFT_OK) return s;
     }
     if (outer_out) *outer_out = outer;
@@ -1903,9 +1948,10 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
 
 // ---- binary FP64 checkpoint (no reference counterpart: the reference keeps
 // only the ASCII win files, scft.cu:785-788).  Layout, host byte order:
-//   "SCFTCKP1" | u32 version (1) | u32 sizeof(scft_problem) | scft_problem
-//   (with the current box) | i32 strn | i64 M | strn x 2M doubles (W-, W+) |
-//   u64 FNV-1a hash of the field bytes
+//   "SCFTCKP1" | u32 version (2) | u32 sizeof(scft_problem) | scft_problem
+//   (with the last common box) | i32 strn | i64 M | strn x 2M doubles
+//   (W-, W+) | strn x 3 doubles (each replica's box) | u64 FNV-1a hash of the
+//   field and box bytes.  Version 1 files (no per-replica boxes) load too.
 namespace {
 constexpr char kCkptMagic[8] = {'S', 'C', 'F', 'T', 'C', 'K', 'P', '1'};
 
@@ -1929,7 +1975,7 @@ scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path)
         ctx->lasterr = "scft_save_checkpoint: cannot open " + tmp;
         return SCFT_BAD_INPUT;
     }
-    const uint32_t ver = 1, psz = sizeof(scft_problem);
+    const uint32_t ver = 2, psz = sizeof(scft_problem);
     const int32_t strn = ctx->strn;
     const int64_t M = ctx->M;
     bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(&ver, 4, 1, f) == 1 && fwrite(&psz, 4, 1, f) == 1 &&
@@ -1946,6 +1992,9 @@ scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path)
         h = fnv1a(h, w.data(), w.size() * sizeof(double));
         ok = fwrite(w.data(), sizeof(double), w.size(), f) == w.size();
     }
+    const size_t nb = 3 * (size_t)ctx->strn;
+    h = fnv1a(h, ctx->Dr.data(), nb * sizeof(double));
+    ok = ok && fwrite(ctx->Dr.data(), sizeof(double), nb, f) == nb;
     ok = ok && fwrite(&h, 8, 1, f) == 1;
     ok = (fclose(f) == 0) && ok;
     if (!ok || std::rename(tmp.c_str(), path) != 0) {
@@ -1975,21 +2024,32 @@ scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path)
     int32_t strn = 0;
     int64_t M = 0;
     if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return fail("not a checkpoint");
-    if (fread(&ver, 4, 1, f) != 1 || ver != 1 || fread(&psz, 4, 1, f) != 1 || psz != sizeof(scft_problem))
+    if (fread(&ver, 4, 1, f) != 1 || (ver != 1 && ver != 2) || fread(&psz, 4, 1, f) != 1 ||
+        psz != sizeof(scft_problem))
         return fail("unsupported version");
     if (fread(&p, psz, 1, f) != 1 || fread(&strn, 4, 1, f) != 1 || fread(&M, 8, 1, f) != 1)
         return fail("truncated header");
     if (strn != ctx->strn || M != ctx->M || p.m[0] != ctx->p.m[0] || p.m[1] != ctx->p.m[1] ||
         p.m[2] != ctx->p.m[2])
         return fail("grid or replica count differs from the context");
-    std::vector<double> all(2 * (size_t)M * strn);
+    std::vector<double> all(2 * (size_t)M * strn), boxes;
     if (fread(all.data(), sizeof(double), all.size(), f) != all.size()) return fail("truncated fields");
+    uint64_t hh = fnv1a(1469598103934665603ull, all.data(), all.size() * sizeof(double));
+    if (ver == 2) {
+        boxes.resize(3 * (size_t)strn);
+        if (fread(boxes.data(), sizeof(double), boxes.size(), f) != boxes.size()) return fail("truncated boxes");
+        hh = fnv1a(hh, boxes.data(), boxes.size() * sizeof(double));
+    }
     uint64_t h = 0;
     if (fread(&h, 8, 1, f) != 1) return fail("truncated hash");
-    if (h != fnv1a(1469598103934665603ull, all.data(), all.size() * sizeof(double))) return fail("hash mismatch");
+    if (h != hh) return fail("hash mismatch");
     fclose(f);
     scft_status s = scft_set_box(ctx, p.D);
     if (s != SCFT_OK) return s;
+    for (int ii = 0; ii < (int)boxes.size() / 3; ii++) {
+        s = scft_set_box_replica(ctx, ii, &boxes[3 * (size_t)ii]);
+        if (s != SCFT_OK) return s;
+    }
     for (int ii = 0; ii < strn; ii++) {
         s = scft_set_fields(ctx, ii, all.data() + (size_t)ii * 2 * M);
         if (s != SCFT_OK) return s;

@@ -144,3 +144,35 @@ def test_checkpointed_adjoint_equals_full_store(built_lib, m, D, N, ens, K, prec
     # the full-store path still works after the checkpointed one reused slot 0
     again, _ = ctx.stress(0)
     np.testing.assert_array_equal(again, full)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_replica_boxes(built_lib, precision):
+    """Every replica owns its box: replica 1 in a 2-replica context with its own
+    box gives the densities and stress of a one-replica context in that box,
+    bit for bit, while replica 0 keeps the common box."""
+    m, N = (12, 8, 16), 24
+    D0, D1 = np.array([3.1, 2.2, 4.0]), np.array([2.9, 2.4, 4.3])
+    wm, wp = smooth_fields(m, D0, 3)
+    two = S.Context(m, D0, N, chi=12, f=0.45, phidb=0.8, ens=1, alpha=0.1, strn=2, dostring=0,
+                    precision=precision)
+    one = S.Context(m, D1, N, chi=12, f=0.45, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0,
+                    precision=precision)
+    for ii in range(2):
+        two.set_fields(ii, wm, wp)
+    one.set_fields(0, wm, wp)
+    two.set_box(D1, ii=1)
+    np.testing.assert_array_equal(two.get_box(1), D1)
+    np.testing.assert_array_equal(two.get_box(0), D0)
+    two.props(1)
+    one.props(0)
+    c2, q2, _ = two.get_conc(1)
+    c1, q1, _ = one.get_conc(0)
+    assert q1 == q2
+    np.testing.assert_array_equal(c1, c2)
+    np.testing.assert_array_equal(two.stress(1)[0], one.stress(0)[0])
+    s0, _ = two.stress(0)
+    ref = S.Context(m, D0, N, chi=12, f=0.45, phidb=0.8, ens=1, alpha=0.1, strn=1, dostring=0,
+                    precision=precision)
+    ref.set_fields(0, wm, wp)
+    np.testing.assert_array_equal(s0, ref.stress(0)[0])

@@ -497,12 +497,50 @@ __device__ __forceinline__ void fft_fwd_mul_inv(cplx<T> *buf, const cplx<T> *tw,
 // Packed z-rows of the fixed shapes sit at an odd stride of M2 + 1 complex
 // elements, so that a warp transforming 32 rows at once (lines fastest) reads
 // and writes 32 different banks; the half spectra [y][kz] keep their natural
-// stride MK2.  The two layouts overlap, so the repack goes through registers
-// with a block-wide barrier between the reads and the writes.
+// stride MK2.  The two layouts overlap in the same buffer: the repack between
+// them happens inside the loads of the first y stage (forward) or the first z
+// stage (inverse), whose barrier separates all reads from all writes.
 template <int M2>
 struct PackedRows {
     static constexpr int LSF = M2 + 1;
 };
+
+// First Stockham stage (NS = 1, no twiddles) whose inputs come from a
+// functor: ld(line, k) returns element k of line `line`.  The outputs go to
+// buf in the stage's usual layout after a barrier, so the functor may read
+// any part of buf (a different layout of the same data) in place.
+template <typename T, int N, int NLINES, int ES, int LS, bool LF, int NT, class Load>
+__device__ __forceinline__ void fft_first_stage_ld(cplx<T> *__restrict__ buf, const cplx<T> *__restrict__ tw,
+                                                   int sign, Load ld)
+{
+    constexpr int R = pick_radix(N);
+    constexpr int NR = N / R, NB = NLINES * NR, PER = (NB + NT - 1) / NT;
+    cplx<T> v[PER][R];
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[i][r] = ld(line, j + r * NR);
+            Dft<T, R>::run(v[i], sign, tw, N);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int b = threadIdx.x + i * NT;
+        if (NB % NT == 0 || b < NB) {
+            const int line = LF ? b % NLINES : b / NR;
+            const int j = LF ? b / NLINES : b % NR;
+            cplx<T> *dst = buf + line * LS + j * R * ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[r * ES] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
 
 // The kz = 0 and kz = M2/2 columns of a slab's half spectrum are real
 // sequences along y before the forward y pass and Hermitian ones before the
@@ -511,45 +549,6 @@ struct PackedRows {
 // e.g. exactly 256 at 64^3) instead of M2/2 + 1.  slab_ysplit_fixed recovers
 // the two spectra after the forward pass: X0(k) = (C(k) + conj C(-k))/2,
 // XH(k) = (C(k) - conj C(-k))/(2i).
-template <typename T, int M1, int M2, int NT>
-__device__ __forceinline__ void slab_unpack_fixed(cplx<T> *buf)
-{
-    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
-    constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
-    cplx<T> A[PER], B[PER];
-#pragma unroll
-    for (int i = 0; i < PER; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (ITEMS % NT == 0 || e < ITEMS) {
-            const int p = e / MK2, kz = e - p * MK2;
-            const cplx<T> ck = buf[p * LS + kz];
-            if (kz == 0) {
-                // rows 2p, 2p+1: (A0, AH) and (B0, BH) are real; packed as c0 + i cH
-                const cplx<T> ch = buf[p * LS + H];
-                A[i] = {ck.x, ch.x};
-                B[i] = {ck.y, ch.y};
-            } else {
-                const cplx<T> cm = buf[p * LS + M2 - kz];
-                A[i] = {(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
-                B[i] = {(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5};
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < PER; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (ITEMS % NT == 0 || e < ITEMS) {
-            const int p = e / MK2, kz = e - p * MK2;
-            if (kz != H) {  // column H is rebuilt by slab_ysplit_fixed
-                buf[2 * p * MK2 + kz] = A[i];
-                if (2 * p + 1 < M1) buf[(2 * p + 1) * MK2 + kz] = B[i];
-            }
-        }
-    }
-    __syncthreads();
-}
-
 // column 0 after the forward y pass holds C = FFT_y(c0 + i cH): split it
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_ysplit_fixed(cplx<T> *buf)
@@ -585,53 +584,27 @@ __device__ __forceinline__ void slab_yjoin_fixed(cplx<T> *buf)
     __syncthreads();
 }
 
-// Inverse of slab_unpack with half-complex-to-real semantics (imaginary parts
-// of the self-conjugate bins dropped); column 0 holds the inverse y pass of
-// c0 + i cH, i.e. the real kz = 0 value in .x and the real kz = M2/2 value in .y.
-template <typename T, int M1, int M2, int NT>
-__device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
-{
-    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
-    constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
-    cplx<T> A[PER], B[PER];
-#pragma unroll
-    for (int i = 0; i < PER; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (ITEMS % NT == 0 || e < ITEMS) {
-            const int p = e / MK2, kz = e - p * MK2;
-            const bool hb = 2 * p + 1 < M1;
-            if (kz == 0 || kz == H) {
-                const cplx<T> a = buf[2 * p * MK2];
-                const cplx<T> b = hb ? buf[(2 * p + 1) * MK2] : cplx<T>{(T)0, (T)0};
-                A[i] = {kz == 0 ? a.x : a.y, (T)0};
-                B[i] = {kz == 0 ? b.x : b.y, (T)0};
-            } else {
-                A[i] = buf[2 * p * MK2 + kz];
-                B[i] = hb ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < PER; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (ITEMS % NT == 0 || e < ITEMS) {
-            const int p = e / MK2, kz = e - p * MK2;
-            buf[p * LS + kz] = {A[i].x - B[i].y, A[i].y + B[i].x};
-            if (kz > 0 && 2 * kz < M2) buf[p * LS + M2 - kz] = {A[i].x + B[i].y, B[i].x - A[i].y};
-        }
-    }
-    __syncthreads();
-}
-
 // packed real rows (stride M2 + 1) -> half spectrum [y][kz]
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
 {
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
-    fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, -1);
-    slab_unpack_fixed<T, M1, M2, NT>(buf);
-    fft_fixed<T, M1, M2 / 2, MK2, 1, true, NT>(buf, twy, -1);
+    constexpr int H = M2 / 2, LSP = PackedRows<M2>::LSF;
+    fft_fixed<T, M2, NPAIR, 1, LSP, true, NT>(buf, twz, -1);
+    // first y stage reads the packed z spectra directly, unpacking per
+    // element: row y = 2p (A) or 2p+1 (B) of column kz
+    fft_first_stage_ld<T, M1, H, MK2, 1, true, NT>(buf, twy, -1, [&](int kz, int y) -> cplx<T> {
+        const cplx<T> *row = buf + (y >> 1) * LSP;
+        const bool odd = y & 1;
+        if (kz == 0) {
+            const cplx<T> c0 = row[0], ch = row[H];
+            return odd ? cplx<T>{c0.y, ch.y} : cplx<T>{c0.x, ch.x};
+        }
+        const cplx<T> ck = row[kz], cm = row[M2 - kz];
+        return odd ? cplx<T>{(ck.y + cm.y) * (T)0.5, (cm.x - ck.x) * (T)0.5}
+                   : cplx<T>{(ck.x + cm.x) * (T)0.5, (ck.y - cm.y) * (T)0.5};
+    });
+    fft_fixed<T, M1, H, MK2, 1, true, NT, pick_radix(M1)>(buf, twy, -1);
     slab_ysplit_fixed<T, M1, M2, NT>(buf);
 }
 
@@ -642,9 +615,27 @@ __device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *
     constexpr int MK2 = M2 / 2 + 1, NPAIR = (M1 + 1) / 2;
     __syncthreads();
     slab_yjoin_fixed<T, M1, M2, NT>(buf);
-    fft_fixed<T, M1, M2 / 2, MK2, 1, true, NT>(buf, twy, +1);
-    slab_pack_fixed<T, M1, M2, NT>(buf);
-    fft_fixed<T, M2, NPAIR, 1, PackedRows<M2>::LSF, true, NT>(buf, twz, +1);
+    constexpr int H = M2 / 2, LSP = PackedRows<M2>::LSF;
+    fft_fixed<T, M1, H, MK2, 1, true, NT>(buf, twy, +1);
+    // first z stage reads the half spectra directly, packing per element:
+    // packed row p at z from rows 2p, 2p+1 at
+    // kz = z or M2 - z; column 0 holds the kz = 0 (.x) and kz = H (.y) values
+    fft_first_stage_ld<T, M2, NPAIR, 1, LSP, true, NT>(buf, twz, +1, [&](int p, int z) -> cplx<T> {
+        const bool hb = 2 * p + 1 < M1;
+        const int kz = z <= H ? z : M2 - z;
+        cplx<T> A, B;
+        if (kz == 0 || kz == H) {
+            const cplx<T> a = buf[2 * p * MK2];
+            const cplx<T> b = hb ? buf[(2 * p + 1) * MK2] : cplx<T>{(T)0, (T)0};
+            A = {kz == 0 ? a.x : a.y, (T)0};
+            B = {kz == 0 ? b.x : b.y, (T)0};
+        } else {
+            A = buf[2 * p * MK2 + kz];
+            B = hb ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
+        }
+        return z <= H ? cplx<T>{A.x - B.y, A.y + B.x} : cplx<T>{A.x + B.y, B.x - A.y};
+    });
+    fft_fixed<T, M2, NPAIR, 1, LSP, true, NT, pick_radix(M2)>(buf, twz, +1);
 }
 
 }  // namespace scft

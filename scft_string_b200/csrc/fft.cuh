@@ -497,9 +497,10 @@ __device__ __forceinline__ void fft_fwd_mul_inv(cplx<T> *buf, const cplx<T> *tw,
 // Packed z-rows of the fixed shapes sit at an odd stride of M2 + 1 complex
 // elements, so that a warp transforming 32 rows at once (lines fastest) reads
 // and writes 32 different banks; the half spectra [y][kz] keep their natural
-// stride MK2.  The two layouts overlap in the same buffer: the repack between
-// them happens inside the loads of the first y stage (forward) or the first z
-// stage (inverse), whose barrier separates all reads from all writes.
+// stride MK2.  The two layouts overlap in the same buffer: the unpack happens
+// inside the loads of the first y stage of the forward transform, whose
+// barrier separates all reads from all writes; the pack before the inverse z
+// pass is a pass of its own (slab_pack_fixed).
 template <int M2>
 struct PackedRows {
     static constexpr int LSF = M2 + 1;
@@ -584,6 +585,47 @@ __device__ __forceinline__ void slab_yjoin_fixed(cplx<T> *buf)
     __syncthreads();
 }
 
+// Half spectra [y][kz] -> packed z-rows (the inverse of the unpack in
+// slab_forward_fixed, with half-complex-to-real semantics: the imaginary
+// parts of the self-conjugate bins are dropped); column 0 holds the kz = 0
+// values in .x and the kz = M2/2 values in .y.  Reads all items into
+// registers, then writes, with a barrier in between (the layouts overlap).
+template <typename T, int M1, int M2, int NT>
+__device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
+{
+    constexpr int MK2 = M2 / 2 + 1, H = M2 / 2, NPAIR = (M1 + 1) / 2, LS = PackedRows<M2>::LSF;
+    constexpr int ITEMS = NPAIR * MK2, PER = (ITEMS + NT - 1) / NT;
+    cplx<T> A[PER], B[PER];
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            const bool hb = 2 * p + 1 < M1;
+            if (kz == 0 || kz == H) {
+                const cplx<T> a = buf[2 * p * MK2];
+                const cplx<T> b = hb ? buf[(2 * p + 1) * MK2] : cplx<T>{(T)0, (T)0};
+                A[i] = {kz == 0 ? a.x : a.y, (T)0};
+                B[i] = {kz == 0 ? b.x : b.y, (T)0};
+            } else {
+                A[i] = buf[2 * p * MK2 + kz];
+                B[i] = hb ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (ITEMS % NT == 0 || e < ITEMS) {
+            const int p = e / MK2, kz = e - p * MK2;
+            buf[p * LS + kz] = {A[i].x - B[i].y, A[i].y + B[i].x};
+            if (kz > 0 && 2 * kz < M2) buf[p * LS + M2 - kz] = {A[i].x + B[i].y, B[i].x - A[i].y};
+        }
+    }
+    __syncthreads();
+}
+
 // packed real rows (stride M2 + 1) -> half spectrum [y][kz]
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
@@ -617,25 +659,10 @@ __device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *
     slab_yjoin_fixed<T, M1, M2, NT>(buf);
     constexpr int H = M2 / 2, LSP = PackedRows<M2>::LSF;
     fft_fixed<T, M1, H, MK2, 1, true, NT>(buf, twy, +1);
-    // first z stage reads the half spectra directly, packing per element:
-    // packed row p at z from rows 2p, 2p+1 at
-    // kz = z or M2 - z; column 0 holds the kz = 0 (.x) and kz = H (.y) values
-    fft_first_stage_ld<T, M2, NPAIR, 1, LSP, true, NT>(buf, twz, +1, [&](int p, int z) -> cplx<T> {
-        const bool hb = 2 * p + 1 < M1;
-        const int kz = z <= H ? z : M2 - z;
-        cplx<T> A, B;
-        if (kz == 0 || kz == H) {
-            const cplx<T> a = buf[2 * p * MK2];
-            const cplx<T> b = hb ? buf[(2 * p + 1) * MK2] : cplx<T>{(T)0, (T)0};
-            A = {kz == 0 ? a.x : a.y, (T)0};
-            B = {kz == 0 ? b.x : b.y, (T)0};
-        } else {
-            A = buf[2 * p * MK2 + kz];
-            B = hb ? buf[(2 * p + 1) * MK2 + kz] : cplx<T>{(T)0, (T)0};
-        }
-        return z <= H ? cplx<T>{A.x - B.y, A.y + B.x} : cplx<T>{A.x + B.y, B.x - A.y};
-    });
-    fft_fixed<T, M2, NPAIR, 1, LSP, true, NT, pick_radix(M2)>(buf, twz, +1);
+    // the pack runs as its own pass: read inside the first z stage (lanes
+    // across packed rows) the half spectra would be 2-way bank conflicts
+    slab_pack_fixed<T, M1, M2, NT>(buf);
+    fft_fixed<T, M2, NPAIR, 1, LSP, true, NT>(buf, twz, +1);
 }
 
 }  // namespace scft

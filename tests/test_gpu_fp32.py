@@ -1,6 +1,6 @@
 """The FP32 propagator path against the FP64 path.
 
-Accuracy is judged at identical fields: the FP64 solver is run to a state,
+Accuracy is measured at identical fields: the FP64 solver is run to a state,
 the same W-, W+ go into an FP32 context, and one props of each gives
 lnQ, rhoA and the free energy per chain F = -lnQ + <chi phiA phiB - wA phiA - wB phiB>
 (scft.cu:820-829).  FP32 storage and transforms have an error floor that grows

@@ -167,6 +167,10 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL);
  * replica ii, for a context created with fcont = 1: the adjoint of the
  * junction step, whose field depends on f.  Either output may be NULL. */
 scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df);
+/* dF/dL_i (3 values), dF/dchiN and dF/df of replica ii in one call (the
+ * gradients entry of the proposed ABI); dF/df needs fcont = 1 and is NaN
+ * otherwise.  Exact at a converged saddle point; any output may be NULL. */
+scft_status scft_gradients(scft_ctx *ctx, int ii, double *dF_dL, double *dF_dchi, double *dF_df);
 scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL,
                              double *bytes_out);
 /* Anderson-accelerated solution of replica ii's field equations (an option

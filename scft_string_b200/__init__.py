@@ -78,6 +78,7 @@ EXPORTS = [
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
     "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
+    "scft_gradients",
 ]
 
 _lib = None
@@ -138,6 +139,7 @@ def lib():
     L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
     L.scft_save_checkpoint.argtypes = [vp, C.c_char_p]
     L.scft_set_box_replica.argtypes = [vp, C.c_int, _dp]
+    L.scft_gradients.argtypes = [vp, C.c_int, _dp, _dp, _dp]
     L.scft_get_box_replica.argtypes = [vp, C.c_int, _dp]
     L.scft_load_checkpoint.argtypes = [vp, C.c_char_p]
     _lib = L
@@ -377,6 +379,13 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self._ck(lib().scft_dF_df(self.h, int(ii), C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def gradients(self, ii=0):
+        """(dF/dL [3], dF/dchiN, dF/df) of replica ii; dF/df is NaN unless fcont=1."""
+        dL = np.zeros(3)
+        dchi, df = C.c_double(), C.c_double()
+        self._ck(lib().scft_gradients(self.h, int(ii), _p(dL), C.byref(dchi), C.byref(df)))
+        return dL, dchi.value, df.value
 
     def dF_dchi(self, ii=0):
         v = C.c_double()

@@ -1686,6 +1686,24 @@ scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
     return SCFT_OK;
 }
 
+// All parameter derivatives of replica ii at its current fields in one call:
+// dF/dL (scft_stress), dF/dchiN (scft_dF_dchi) and, for a continuous A
+// fraction, dF/df (scft_dF_df); dF/df is NaN otherwise (f enters the
+// reference discretisation only through the integer n1).
+scft_status scft_gradients(scft_ctx *ctx, int ii, double *dF_dL, double *dF_dchi, double *dF_df)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    scft_status s = scft_stress(ctx, ii, nullptr, dF_dL);
+    if (s == SCFT_OK && dF_dchi) s = scft_dF_dchi(ctx, ii, dF_dchi);
+    if (s == SCFT_OK && dF_df) {
+        if (ctx->g.jon)
+            s = scft_dF_df(ctx, ii, nullptr, dF_df);
+        else
+            *dF_df = std::nan("");
+    }
+    return s;
+}
+
 // Anderson-accelerated solution of replica ii's field equations (no
 // reference counterpart; the reference keeps only its scaffolding,
 // scft.cu:30-31): residual d = (chi (phiB - phiA) - 2 W-, chi (phiA + phiB - 1))

@@ -121,3 +121,19 @@ def test_saddle_point_dF_df(built_lib):
     fd = (Fp - Fm) / (2 * h)
     print("dF/df adjoint", dF, "fd", fd, "rel", abs(dF - fd) / abs(fd))
     assert abs(dF - fd) <= 2e-3 * max(1.0, abs(fd))
+
+
+def test_gradients_entry_point(built_lib):
+    """scft_gradients returns what the individual derivative calls return."""
+    m, D, N = (8, 12, 10), np.array([2.0, 3.0, 2.5]), 20
+    wm, wp = _fields(m, D, 7)
+    for fcont in (0, 1):
+        ctx = _ctx(m, D, N, 0.47, 1, fcont=fcont)
+        ctx.set_fields(0, wm, wp)
+        dL, dchi, df = ctx.gradients(0)
+        np.testing.assert_array_equal(dL, ctx.stress(0)[1])
+        assert dchi == ctx.dF_dchi(0)
+        if fcont:
+            assert df == ctx.dF_df(0)[1]
+        else:
+            assert np.isnan(df)

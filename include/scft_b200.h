@@ -171,6 +171,14 @@ scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df);
  * gradients entry of the proposed ABI); dF/df needs fcont = 1 and is NaN
  * otherwise.  Exact at a converged saddle point; any output may be NULL. */
 scft_status scft_gradients(scft_ctx *ctx, int ii, double *dF_dL, double *dF_dchi, double *dF_df);
+/* density::props of replica ii (the same results as scft_props, up to the
+ * order of the FP64 sums) with the propagators held only at checkpoints at
+ * most K contour steps apart: a forward pass keeps the checkpoints, then every
+ * segment is recomputed once next to its mirror segment and the Simpson terms
+ * q(s) q^dagger(N-s) are accumulated per point.  Device memory: *bytes_out
+ * (may be NULL); the context's full store is not touched.  lnQ_out and
+ * phis_out[5] as scft_get_conc (either may be NULL). */
+scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out);
 scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL,
                              double *bytes_out);
 /* Anderson-accelerated solution of replica ii's field equations (an option

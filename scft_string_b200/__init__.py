@@ -78,7 +78,7 @@ EXPORTS = [
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
     "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
-    "scft_gradients",
+    "scft_gradients", "scft_props_ckpt",
 ]
 
 _lib = None
@@ -140,6 +140,7 @@ def lib():
     L.scft_save_checkpoint.argtypes = [vp, C.c_char_p]
     L.scft_set_box_replica.argtypes = [vp, C.c_int, _dp]
     L.scft_gradients.argtypes = [vp, C.c_int, _dp, _dp, _dp]
+    L.scft_props_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_get_box_replica.argtypes = [vp, C.c_int, _dp]
     L.scft_load_checkpoint.argtypes = [vp, C.c_char_p]
     _lib = L
@@ -350,6 +351,15 @@ class Context:
         a, b = np.zeros(3), np.zeros(3)
         self._ck(lib().scft_stress(self.h, int(ii), _p(a), _p(b)))
         return a, b
+
+    def props_ckpt(self, ii=0, K=13):
+        """density::props of replica ii with propagators kept every K steps;
+        returns (lnQ, phis, device bytes); densities as get_conc(ii)."""
+        q = C.c_double()
+        phis = np.zeros(5)
+        nb = C.c_double()
+        self._ck(lib().scft_props_ckpt(self.h, int(ii), int(K), C.byref(q), _p(phis), C.byref(nb)))
+        return q.value, phis, nb.value
 
     def stress_ckpt(self, ii=0, K=13):
         """(d lnQ/dL, dF/dL, device bytes) by the adjoint with checkpoints K steps apart."""

@@ -12,7 +12,8 @@ LIB = os.path.join(HERE, "libscft_b200.so")
 EXE = os.path.join(HERE, "scft_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu", "noalloc.cu",
+              "density_ckpt.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh"]
 
 

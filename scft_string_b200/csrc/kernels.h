@@ -122,6 +122,24 @@ int launch_junction_dtheta(const StressArgs<T> &a, const StressPairs &P, int sla
                            int pencil_threads, int pencil_smem, double *part, int nblk, double *out,
                            cudaStream_t st);
 
+// ------------------------------------------------------------------ checkpointed densities
+constexpr int kDensPairs = 32;
+
+// slice pairs of one accumulation launch: element offsets (from the launch's
+// base pointer) of q(s) and q^dagger(N-s) (or q^dagger(j), q^dagger(Nh-j)),
+// and the raw Simpson weight of the product in the A block, the B block and
+// the homopolymer sum
+struct DensPairs {
+    int n;
+    long long x[kDensPairs], y[kDensPairs];
+    double wA[kDensPairs], wB[kDensPairs], wH[kDensPairs];
+};
+
+template <typename T>
+int launch_density_acc(const T *base, size_t M, const DensPairs &P, double *acc, int nblk, cudaStream_t st);
+int launch_density_final(const double *acc, size_t M, double *rs_row, double ds, double chi, double *conc,
+                         double *part, int nblk, cudaStream_t st);
+
 // ------------------------------------------------------------------ FP64 field kernels
 constexpr int kMaxStrn = 64;
 

@@ -1457,37 +1457,69 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
     return SCFT_OK;
 }
 
-// The same adjoint with the propagators stored only at checkpoints.
-// Positions: the starts of a mirror-symmetric partition of [0, N) into pieces
-// of at most K steps (and of [0, Nh) for the homopolymer pairs).  A forward
-// pass over the whole chain keeps those slices plus q(N) and q^dagger(Nh)
-// (for QC and Q2).  Then each piece [a, b) is recomputed together with its
-// mirror [N-b, N-a): the two segments hold q(s) and q^dagger(N-1-s) for every
-// s of both pieces, i.e. all of their pairs.  Cost: two chain passes; memory:
-// (#checkpoints + 2 (K+1) + 2) slice pairs instead of N+1.  The slices are the
-// same bits as the full store's (same kernels, same inputs), so the result
-// equals scft_stress up to the order of the final FP64 pair sums.
-scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL, double *bytes_out)
+}  // extern "C"
+
+namespace {
+
+// Propagators of one replica held only at checkpoints (the checkpointed
+// adjoint and density pass).  Positions: the starts of a mirror-symmetric
+// partition of [0, N) into pieces of at most K steps, and of [0, Nh) for the
+// homopolymer.  ck_mem holds, in slice pairs (q, q^dagger): the checkpoints,
+// two segments of K+1 slices, [q^dagger(Nh), q(N)], then `extra` bytes.
+struct CkptRun {
+    int K = 0;
+    std::vector<int> bc, bh, row_of, pos;
+    size_t pairB = 0;
+    unsigned char *ck = nullptr, *seg = nullptr, *segB = nullptr, *qb = nullptr, *extra = nullptr;
+    double bytes = 0;
+};
+
+template <typename T>
+PropsArgs<T> ckpt_args(scft_ctx *ctx, const Geo &gg, void *hist)
 {
-    if (!ctx || ii < 0 || ii >= ctx->strn || K < 1) return SCFT_BAD_INPUT;
+    PropsArgs<T> a = props_args_from<T>(ctx, ctx->rep_dev, 0);
+    a.g = gg;
+    a.hist = (T *)hist;
+    return a;
+}
+
+// g.Ns = len steps of slot 0 from contour index p0 (segment Geo: n1, n2 and the
+// junction steps shifted by p0), starting from store slice 0 (mode 2) or q = 1
+void ckpt_chain(scft_ctx *ctx, int p0, int len, void *buf, int first_mode)
+{
+    const Geo &g = ctx->g;
+    Geo gg = g;
+    gg.Ns = len;
+    gg.n1 = g.n1 - p0;
+    gg.n2 = g.n2 - p0;
+    gg.jq = g.jq - p0;
+    gg.jqd = g.jqd - p0;
+    ctx->stats.kernel_launches += ctx->prec == SCFT_FP32
+                                      ? launch_chain<float>(ckpt_args<float>(ctx, gg, buf), ctx->L, first_mode, ctx->st)
+                                      : launch_chain<double>(ckpt_args<double>(ctx, gg, buf), ctx->L, first_mode, ctx->st);
+}
+
+// allocation, forward pass (checkpoints, q^dagger(Nh), q(N)), then Q2, QC,
+// lnQ and the ensemble weights of replica ii in rs (device and rs_h)
+scft_status ckpt_forward(scft_ctx *ctx, int ii, int K, size_t extra_bytes, CkptRun &R)
+{
     const Geo &g = ctx->g;
     const int N = g.Ns, Nh = g.Nh;
-    K = std::min(K, N);
-    scft_status s = stress_alloc(ctx);
-    if (s != SCFT_OK) return s;
-    const std::vector<int> bc = mirror_bounds(N, K);
-    const std::vector<int> bh = Nh > 0 ? mirror_bounds(Nh, std::min(K, Nh)) : std::vector<int>{0};
-    // checkpoint rows: every piece start of both partitions
-    std::vector<int> row_of(N + 1, -1), pos;
-    for (size_t k = 0; k + 1 < bc.size(); k++) pos.push_back(bc[k]);
-    for (size_t k = 0; k + 1 < bh.size(); k++) pos.push_back(bh[k]);
-    std::sort(pos.begin(), pos.end());
-    pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
-    for (size_t r = 0; r < pos.size(); r++) row_of[pos[r]] = (int)r;
+    R.K = K = std::min(K, N);
+    R.bc = mirror_bounds(N, K);
+    R.bh = Nh > 0 ? mirror_bounds(Nh, std::min(K, Nh)) : std::vector<int>{0};
+    R.row_of.assign(N + 1, -1);
+    R.pos.clear();
+    for (size_t k = 0; k + 1 < R.bc.size(); k++) R.pos.push_back(R.bc[k]);
+    for (size_t k = 0; k + 1 < R.bh.size(); k++) R.pos.push_back(R.bh[k]);
+    R.pos.push_back(0);
+    std::sort(R.pos.begin(), R.pos.end());
+    R.pos.erase(std::unique(R.pos.begin(), R.pos.end()), R.pos.end());
+    for (size_t r = 0; r < R.pos.size(); r++) R.row_of[R.pos[r]] = (int)r;
     const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
-    const size_t pairB = 2 * (size_t)g.M * T;  // one slice pair (q, q^dagger)
-    const size_t nrow = pos.size() + 2 * (size_t)(K + 1) + 2;
-    const size_t need = nrow * pairB;
+    R.pairB = 2 * (size_t)g.M * T;
+    const size_t nrow = R.pos.size() + 2 * (size_t)(K + 1) + 2;
+    const size_t need = nrow * R.pairB + extra_bytes;
     if (ctx->ck_bytes < need) {
         if (ctx->ck_mem) cudaFree(ctx->ck_mem);
         ctx->ck_mem = nullptr;
@@ -1495,75 +1527,83 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
         CK(cudaMalloc(&ctx->ck_mem, need));
         ctx->ck_bytes = need;
     }
-    unsigned char *ck = (unsigned char *)ctx->ck_mem;        // [pos.size()] checkpoint pairs
-    unsigned char *seg = ck + pos.size() * pairB;             // segment A (K+1), segment B (K+1)
-    unsigned char *segB = seg + (size_t)(K + 1) * pairB;
-    unsigned char *qb = segB + (size_t)(K + 1) * pairB;       // [q^dagger(Nh) pair, q(N) pair]
-    if (bytes_out) *bytes_out = (double)need;
-
-    s = upload_list(ctx, {ii});
+    R.ck = (unsigned char *)ctx->ck_mem;
+    R.seg = R.ck + R.pos.size() * R.pairB;
+    R.segB = R.seg + (size_t)(K + 1) * R.pairB;
+    R.qb = R.segB + (size_t)(K + 1) * R.pairB;
+    R.extra = R.qb + 2 * R.pairB;
+    R.bytes = (double)need;
+    scft_status s = upload_list(ctx, {ii});
     if (s != SCFT_OK) return s;
     for (auto &so : ctx->slot_of)  // slot 0's E tables and spectra are reused below
         if (so == 0) so = -1;
     const bool f32 = ctx->prec == SCFT_FP32;
-    auto args_f = [&](Geo gg, void *hist) {
-        PropsArgs<float> a = props_args_from<float>(ctx, ctx->rep_dev, 0);
-        a.g = gg;
-        a.hist = (float *)hist;
-        return a;
-    };
-    auto args_d = [&](Geo gg, void *hist) {
-        PropsArgs<double> a = props_args_from<double>(ctx, ctx->rep_dev, 0);
-        a.g = gg;
-        a.hist = (double *)hist;
-        return a;
-    };
-    auto chain = [&](int p0, int len, void *buf, int first_mode) {
-        Geo gg = g;
-        gg.Ns = len;
-        gg.n1 = g.n1 - p0;
-        gg.n2 = g.n2 - p0;
-        gg.jq = g.jq - p0;
-        gg.jqd = g.jqd - p0;
-        ctx->stats.kernel_launches += f32 ? launch_chain<float>(args_f(gg, buf), ctx->L, first_mode, ctx->st)
-                                          : launch_chain<double>(args_d(gg, buf), ctx->L, first_mode, ctx->st);
-    };
     auto cp = [&](void *dst, const void *src) {
-        return cudaMemcpyAsync(dst, src, pairB, cudaMemcpyDeviceToDevice, ctx->st);
+        return cudaMemcpyAsync(dst, src, R.pairB, cudaMemcpyDeviceToDevice, ctx->st);
     };
-    // forward pass: E tables of replica ii in slot 0, then the chain piece by piece
-    ctx->stats.kernel_launches += f32 ? launch_prepare<float>(args_f(g, ctx->hist), ctx->L, ctx->st)
-                                      : launch_prepare<double>(args_d(g, ctx->hist), ctx->L, ctx->st);
-    std::vector<int> stops(pos);
+    // E tables of replica ii in slot 0, then the chain piece by piece
+    ctx->stats.kernel_launches += f32 ? launch_prepare<float>(ckpt_args<float>(ctx, g, ctx->hist), ctx->L, ctx->st)
+                                      : launch_prepare<double>(ckpt_args<double>(ctx, g, ctx->hist), ctx->L, ctx->st);
+    std::vector<int> stops(R.pos);
     stops.push_back(N);
     if (Nh > 0 && Nh < N) stops.push_back(Nh);
     std::sort(stops.begin(), stops.end());
     stops.erase(std::unique(stops.begin(), stops.end()), stops.end());
     int prev = 0;  // length of the previous piece: its last slice starts the next one
+    unsigned char *seg = R.seg;
     for (size_t k = 0; k + 1 < stops.size(); k++) {
         const int p0 = stops[k], p1 = stops[k + 1];
-        if (p0 > 0) CK(cp(seg, seg + (size_t)prev * pairB));
-        chain(p0, p1 - p0, seg, p0 == 0 ? 1 : 2);
+        if (p0 > 0) CK(cp(seg, seg + (size_t)prev * R.pairB));
+        ckpt_chain(ctx, p0, p1 - p0, seg, p0 == 0 ? 1 : 2);
         prev = p1 - p0;
-        if (p0 == 0) CK(cp(ck + row_of[0] * pairB, seg));
-        if (p0 == 0 && Nh == 0) CK(cp(qb, seg));
-        if (p1 < N && row_of[p1] >= 0) CK(cp(ck + row_of[p1] * pairB, seg + (size_t)(p1 - p0) * pairB));
-        if (p1 == Nh) CK(cp(qb, seg + (size_t)(p1 - p0) * pairB));
-        if (p1 == N) CK(cp(qb + pairB, seg + (size_t)(p1 - p0) * pairB));
+        if (p0 == 0) CK(cp(R.ck + R.row_of[0] * R.pairB, seg));
+        if (p0 == 0 && Nh == 0) CK(cp(R.qb, seg));
+        if (p1 < N && R.row_of[p1] >= 0) CK(cp(R.ck + R.row_of[p1] * R.pairB, seg + (size_t)(p1 - p0) * R.pairB));
+        if (p1 == Nh) CK(cp(R.qb, seg + (size_t)(p1 - p0) * R.pairB));
+        if (p1 == N) CK(cp(R.qb + R.pairB, seg + (size_t)(p1 - p0) * R.pairB));
     }
     CK(cudaGetLastError());
     // Q2 = <q^dagger(Nh)>, QC = <q(N)>: a two-slice store with Ns = 1, Nh = 0
-    {
-        Geo gq = g;
-        gq.Ns = 1;
-        gq.Nh = 0;
-        ctx->stats.kernel_launches += f32 ? launch_qsums<float>(args_f(gq, qb), ctx->L, ctx->st)
-                                          : launch_qsums<double>(args_d(gq, qb), ctx->L, ctx->st);
-        CK(cudaMemcpyAsync(&ctx->rs_h[(size_t)ii * kRsStride], ctx->rs + (size_t)ii * kRsStride,
-                           sizeof(double) * kRsStride, cudaMemcpyDeviceToHost, ctx->st));
-        s = check_device_err(ctx);
-        if (s != SCFT_OK) return s;
-    }
+    Geo gq = g;
+    gq.Ns = 1;
+    gq.Nh = 0;
+    ctx->stats.kernel_launches += f32 ? launch_qsums<float>(ckpt_args<float>(ctx, gq, R.qb), ctx->L, ctx->st)
+                                      : launch_qsums<double>(ckpt_args<double>(ctx, gq, R.qb), ctx->L, ctx->st);
+    CK(cudaMemcpyAsync(&ctx->rs_h[(size_t)ii * kRsStride], ctx->rs + (size_t)ii * kRsStride,
+                       sizeof(double) * kRsStride, cudaMemcpyDeviceToHost, ctx->st));
+    return check_device_err(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+// The same adjoint with the propagators stored only at checkpoints (CkptRun).
+// Each piece [a, b) is recomputed together with its mirror [N-b, N-a): the two
+// segments hold q(s) and q^dagger(N-1-s) for every s of both pieces, i.e. all
+// of their pairs.  Cost: two chain passes; memory: (#checkpoints + 2 (K+1) + 2)
+// slice pairs instead of N+1.  The slices are the same bits as the full
+// store's (same kernels, same inputs), so the result equals scft_stress up to
+// the order of the final FP64 pair sums.
+scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL, double *bytes_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || K < 1) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    const int N = g.Ns, Nh = g.Nh;
+    scft_status s = stress_alloc(ctx);
+    if (s != SCFT_OK) return s;
+    CkptRun R;
+    s = ckpt_forward(ctx, ii, K, 0, R);
+    if (s != SCFT_OK) return s;
+    K = R.K;
+    if (bytes_out) *bytes_out = R.bytes;
+    const size_t pairB = R.pairB;
+    unsigned char *ck = R.ck, *seg = R.seg, *segB = R.segB;
+    const std::vector<int> &bc = R.bc, &bh = R.bh, &row_of = R.row_of;
+    auto cp = [&](void *dst, const void *src) {
+        return cudaMemcpyAsync(dst, src, pairB, cudaMemcpyDeviceToDevice, ctx->st);
+    };
+    auto chain = [&](int p0, int len, void *buf, int first_mode) { ckpt_chain(ctx, p0, len, buf, first_mode); };
     const double Q2 = rsv(ctx, ii, kRsQ2), QC = rsv(ctx, ii, kRsQC);
     double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0};
     // recompute each piece with its mirror; the pairs of both pieces
@@ -1611,6 +1651,129 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
         if (s != SCFT_OK) return s;
     }
     stress_finish(ctx, Q2, QC, dQC, dQ2, dlnQ_dL, dF_dL);
+    return SCFT_OK;
+}
+
+// density::props of replica ii (density.h:344-459) with the propagators held
+// only at checkpoints (CkptRun): the forward pass gives Q2, QC, lnQ and the
+// ensemble weights; each piece [a, b) of [0, N) recomputed with its mirror
+// [N-b, N-a) holds q(s) and q^dagger(N-s) for every s of both pieces, whose
+// products are Kahan-accumulated per point with the reference's Simpson
+// weights (1 at s = 0, n1, N; 4, 2, 4, ... restarting after each block end;
+// no odd-count correction), and likewise q^dagger(j) q^dagger(Nh-j) for the
+// homopolymer.  Writes the replica's densities and phis as scft_props does;
+// the context's full store is not touched.  Equal to scft_props up to the
+// order of the FP64 sums.
+scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out)
+{
+    if (!ctx || ii < 0 || ii >= ctx->strn || K < 1) return SCFT_BAD_INPUT;
+    const Geo &g = ctx->g;
+    const int N = g.Ns, Nh = g.Nh, n1 = g.n1;
+    const size_t M = g.M, T = ctx->prec == SCFT_FP32 ? 4 : 8;
+    CkptRun R;
+    scft_status s = ckpt_forward(ctx, ii, K, 6 * M * sizeof(double), R);
+    if (s != SCFT_OK) return s;
+    if (bytes_out) *bytes_out = R.bytes;
+    double *acc = reinterpret_cast<double *>(R.extra);
+    CK(cudaMemsetAsync(acc, 0, 6 * M * sizeof(double), ctx->st));
+    // raw Simpson weights (density.h:404-422; the continuous A fraction moves
+    // theta of the junction step's trapezoid weight from B to A)
+    auto wA = [&](int t) {
+        double w = (t == 0) + (t == n1);
+        if (t > 0 && t < n1) w += ((t - 1) & 1) ? 2 : 4;
+        if (g.jon && (t == n1 || t == n1 + 1)) w += 1.5 * g.theta;
+        return w;
+    };
+    auto wB = [&](int t) {
+        double w = (t == n1) + (t == N);
+        if (t > n1 && t < N) w += ((t - n1 - 1) & 1) ? 2 : 4;
+        if (g.jon && (t == n1 || t == n1 + 1)) w -= 1.5 * g.theta;
+        return w;
+    };
+    auto wH = [&](int j) {
+        double w = (j == 0) + (j == Nh);
+        if (j > 0 && j < Nh) w += ((j - 1) & 1) ? 2 : 4;
+        return w;
+    };
+    // element offset of slice `sl`, field `fld` of a slice-pair buffer inside ck_mem
+    auto off = [&](const unsigned char *buf, int sl, int fld) {
+        return (long long)((buf - R.ck) / T) + (long long)sl * 2 * (long long)M + (long long)fld * (long long)M;
+    };
+    DensPairs P;
+    std::memset(&P, 0, sizeof(P));
+    auto flush = [&]() {
+        if (P.n == 0) return;
+        ctx->stats.kernel_launches += T == 4 ? launch_density_acc<float>((const float *)R.ck, M, P, acc,
+                                                                         ctx->L.red_blocks, ctx->st)
+                                             : launch_density_acc<double>((const double *)R.ck, M, P, acc,
+                                                                          ctx->L.red_blocks, ctx->st);
+        P.n = 0;
+    };
+    auto add = [&](long long x, long long y, double a, double b, double h) {
+        if (P.n == kDensPairs) flush();
+        P.x[P.n] = x;
+        P.y[P.n] = y;
+        P.wA[P.n] = a;
+        P.wB[P.n] = b;
+        P.wH[P.n] = h;
+        P.n++;
+    };
+    auto cp = [&](void *dst, const void *src) {
+        return cudaMemcpyAsync(dst, src, R.pairB, cudaMemcpyDeviceToDevice, ctx->st);
+    };
+    // pieces with their mirrors: products x(t) y(n - t), x in field fx, y in field 1
+    auto sweep = [&](const std::vector<int> &b, int n, bool homo) -> scft_status {
+        for (size_t k = 0; k + 1 < b.size(); k++) {
+            const int a0 = b[k], a1 = b[k + 1], m0 = n - a1, m1 = n - a0;
+            if (a0 > m0) continue;  // right half: done as a mirror
+            const bool self = (a0 == m0);
+            cudaError_t e = cp(R.seg, R.ck + R.row_of[a0] * R.pairB);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "checkpoint copy");
+            ckpt_chain(ctx, a0, a1 - a0, R.seg, 2);
+            if (!self) {
+                e = cp(R.segB, R.ck + R.row_of[m0] * R.pairB);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "checkpoint copy");
+                ckpt_chain(ctx, m0, m1 - m0, R.segB, 2);
+            }
+            const unsigned char *mir = self ? R.seg : R.segB;  // holds slices m0 .. m1
+            const int fx = homo ? 1 : 0;
+            for (int t = a0; t < a1; t++) {  // y(n - t) in (m0, m1]
+                const int u = n - t;
+                add(off(R.seg, t - a0, fx), off(mir, u - m0, 1), homo ? 0 : wA(t), homo ? 0 : wB(t), homo ? wH(t) : 0);
+            }
+            if (!self)
+                for (int t = m0; t < m1; t++) {  // y(n - t) in (a0, a1]
+                    const int u = n - t;
+                    add(off(R.segB, t - m0, fx), off(R.seg, u - a0, 1), homo ? 0 : wA(t), homo ? 0 : wB(t),
+                        homo ? wH(t) : 0);
+                }
+            flush();  // the next piece overwrites the segments
+        }
+        return SCFT_OK;
+    };
+    s = sweep(R.bc, N, false);
+    if (s != SCFT_OK) return s;
+    if (Nh > 0) {
+        s = sweep(R.bh, Nh, true);
+        if (s != SCFT_OK) return s;
+    }
+    // end points: q(N) q^dagger(0) and q^dagger(Nh) q^dagger(0) (slice 0 is the
+    // first checkpoint; q(N) and q^dagger(Nh) were kept by the forward pass)
+    const unsigned char *c0 = R.ck + R.row_of[0] * R.pairB;
+    add(off(R.qb + R.pairB, 0, 0), off(c0, 0, 1), wA(N), wB(N), 0);
+    add(off(R.qb, 0, 1), off(c0, 0, 1), 0, 0, wH(Nh));
+    flush();
+    ctx->stats.kernel_launches += launch_density_final(acc, M, ctx->rs + (size_t)ii * kRsStride, 1.0 / N,
+                                                       ctx->p.chi, ctx->conc + (size_t)ii * 4 * M, ctx->partials,
+                                                       ctx->L.red_blocks, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&ctx->rs_h[(size_t)ii * kRsStride], ctx->rs + (size_t)ii * kRsStride,
+                       sizeof(double) * kRsStride, cudaMemcpyDeviceToHost, ctx->st));
+    s = check_device_err(ctx);
+    if (s != SCFT_OK) return s;
+    if (lnQ_out) *lnQ_out = rsv(ctx, ii, kRsLnQ);
+    if (phis_out)
+        for (int k = 0; k < 5; k++) phis_out[k] = rsv(ctx, ii, kRsPhis + k);
     return SCFT_OK;
 }
 

@@ -176,3 +176,34 @@ def test_replica_boxes(built_lib, precision):
                     precision=precision)
     ref.set_fields(0, wm, wp)
     np.testing.assert_array_equal(s0, ref.stress(0)[0])
+
+
+@pytest.mark.parametrize("m,D,N,f,ens,K,prec,fcont", [
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.45, 1, 3, "fp64", 0),    # odd A block
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.45, 2, 1, "fp64", 0),    # every slice a checkpoint
+    ((12, 8, 16), (3.1, 2.2, 4.0), 24, 0.43, 1, 5, "fp64", 1),    # junction step inside the chain
+    ((32, 32, 32), (4.0, 4.0, 4.0), 40, 0.5, 2, 7, "fp32", 0),    # compile-time shape
+    ((64, 64, 96), (4.2, 4.2, 6.3), 160, 0.4, 1, 13, "fp32", 0),  # 64x64x96, N=160, every 13 steps
+])
+def test_checkpointed_density_equals_props(built_lib, m, D, N, f, ens, K, prec, fcont):
+    """The density pass from checkpoints (segments recomputed with their
+    mirrors, Simpson terms accumulated per point) gives the densities, lnQ and
+    phis of the full-store props: the slices are the same bits, only the FP64
+    sums run in another order."""
+    D = np.array(D)
+    wm, wp = smooth_fields(m, D, 4)
+    ctx = S.Context(m, D, N, chi=12, f=f, phidb=0.8, ens=ens, alpha=0.1, strn=1, dostring=0,
+                    precision=prec, fcont=fcont)
+    ctx.set_fields(0, wm, wp)
+    ctx.props(0)
+    c0, q0, p0 = ctx.get_conc(0)
+    q1, p1, nbytes = ctx.props_ckpt(0, K)
+    c1, q2, p2 = ctx.get_conc(0)
+    assert q1 == q2 and np.array_equal(p1, p2)
+    assert abs(q1 - q0) <= 1e-13 * abs(q0)
+    np.testing.assert_allclose(p1, p0, rtol=1e-12, atol=1e-15)
+    assert np.abs(c1 - c0).max() <= 1e-12 * np.abs(c0).max()
+    store = (N + 1) * 2 * ctx.M * (4 if prec == "fp32" else 8)
+    if 3 <= K < N:
+        assert nbytes < store + 6 * 8 * ctx.M
+    print(m, N, K, prec, "checkpointed density bytes", nbytes, "full store", store)

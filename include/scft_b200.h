@@ -60,6 +60,13 @@ typedef struct {
                          * reference counterpart): n1 = floor(N f) whole A steps, and step
                          * n1 sees the field theta wA + (1-theta) wB, theta = N f - n1, with
                          * theta of its Simpson weight moved from B to A; needs Nh < N - n1 */
+    int    nostore;     /* 0: every props keeps all N+1 propagator slices (the reference's
+                         * dev_qq).  1: no full store: props runs from checkpoints every ckpt_K
+                         * contour steps (scft_props_ckpt), one replica at a time, about twice
+                         * the work in a fraction of the memory; scft_stress uses the
+                         * checkpointed adjoint; scft_do_step, scft_get_propagator and
+                         * scft_dF_df return SCFT_UNSUPPORTED */
+    int    ckpt_K;      /* checkpoint interval with nostore (0: ceil(sqrt(N))) */
 } scft_problem;
 
 typedef struct scft_ctx scft_ctx;

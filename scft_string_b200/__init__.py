@@ -53,6 +53,8 @@ class Problem(C.Structure):
         ("batched", C.c_int),
         ("device", C.c_int),
         ("fcont", C.c_int),
+        ("nostore", C.c_int),
+        ("ckpt_K", C.c_int),
     ]
 
 
@@ -163,7 +165,8 @@ class Context:
     """An scft_ctx: every replica of one problem resident on one B200."""
 
     def __init__(self, m, D, N, chi, f, phidb, ens=2, alpha=0.1, strn=1, fix=(0, 0),
-                 dostring=1, springsteps=0, precision="fp64", batched=True, device=0, fcont=0):
+                 dostring=1, springsteps=0, precision="fp64", batched=True, device=0, fcont=0, nostore=0,
+                 ckpt_K=0):
         p = Problem()
         p.m = (C.c_int * 3)(*[int(v) for v in m])
         p.D = (C.c_double * 3)(*[float(v) for v in D])
@@ -175,6 +178,8 @@ class Context:
         p.batched = 1 if batched else 0
         p.device = int(device)
         p.fcont = int(fcont)
+        p.nostore = int(nostore)
+        p.ckpt_K = int(ckpt_K)
         self.problem = p
         self.m = tuple(int(v) for v in m)
         self.M = int(np.prod(self.m))
@@ -446,4 +451,4 @@ def StringSolver(cfg: dict, precision="fp64", batched=True, springsteps=0, devic
                    ens=cfg["ens"], alpha=cfg.get("alpha", 0.1), strn=cfg["strn"],
                    fix=cfg.get("fix", (0, 0)), dostring=cfg.get("dostring", 1),
                    springsteps=springsteps, precision=precision, batched=batched, device=device,
-                   fcont=cfg.get("fcont", 0))
+                   fcont=cfg.get("fcont", 0), nostore=cfg.get("nostore", 0), ckpt_K=cfg.get("ckpt_K", 0))

@@ -92,6 +92,8 @@ struct scft_ctx {
     int and_H = 0;
     double *st_part = nullptr, *st_out = nullptr;
     void *jd_rbuf = nullptr;  // junction derivative: six real work arrays
+    bool nostore = false;    // props from checkpoints, no full propagator store
+    int ckK = 0;             // checkpoint interval of the nostore props
     void *ck_mem = nullptr;  // checkpointed adjoint: checkpoints, two segments, Q slices
     size_t ck_bytes = 0;
     int rt_slab_threads = 0, rt_slab_smem = 0, rt_pencil_threads = 0, rt_pencil_smem = 0;
@@ -216,10 +218,32 @@ scft_status upload_list(scft_ctx *ctx, const std::vector<int> &reps)
     return SCFT_OK;
 }
 
-// density::props for a list of replicas; scalars land in ctx->rs_h
+scft_status props_ckpt_impl(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out);
+
+// density::props for a list of replicas; scalars land in ctx->rs_h.  Without a
+// full store (nostore) each replica runs from checkpoints.
 scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
 {
     if (reps.empty()) return SCFT_OK;
+    if (ctx->nostore) {
+        CK(cudaEventRecord(ctx->ev0, ctx->st));
+        for (int r : reps) {
+            scft_status s = props_ckpt_impl(ctx, r, ctx->ckK, nullptr, nullptr, nullptr);
+            if (s != SCFT_OK) return s;
+            ctx->slot_of[r] = -1;
+        }
+        CK(cudaEventRecord(ctx->ev1, ctx->st));
+        CK(cudaMemcpyAsync(ctx->rs_h.data(), ctx->rs, sizeof(double) * ctx->rs_h.size(), cudaMemcpyDeviceToHost,
+                           ctx->st));
+        scft_status s = check_device_err(ctx);
+        if (s != SCFT_OK) return s;
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        ctx->stats.props_seconds += ms * 1e-3;
+        ctx->stats.props_calls += (long long)reps.size();
+        ctx->stats.contour_steps += (long long)reps.size() * ctx->g.Ns;
+        return SCFT_OK;
+    }
     scft_status s = upload_list(ctx, reps);
     if (s != SCFT_OK) return s;
     CK(cudaEventRecord(ctx->ev0, ctx->st));
@@ -612,7 +636,9 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
     ctx->M = g.M;
     ctx->Mk = g.Mk;
     ctx->nrep_alloc = p->strn + 1;  // + one scratch replica for scft_props_host
-    ctx->nslots = p->batched ? p->strn : 1;
+    ctx->nostore = p->nostore != 0;
+    ctx->ckK = p->ckpt_K > 0 ? p->ckpt_K : (int)std::ceil(std::sqrt((double)p->N));
+    ctx->nslots = (p->batched && !ctx->nostore) ? p->strn : 1;
     const size_t T = p->precision == SCFT_FP32 ? 4 : 8;
 
     // launch geometry
@@ -692,7 +718,8 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMalloc(&ctx->err, sizeof(int)));
         CKC(cudaMalloc(&ctx->etab, T * 2 * M * S));
         if (g.jon) CKC(cudaMalloc(&ctx->jtab, T * M * S));
-        CKC(cudaMalloc(&ctx->hist, T * 2 * M * (size_t)(g.Ns + 1) * S));
+        // the full propagator store (2 slices per step and slot); a stub without it
+        CKC(cudaMalloc(&ctx->hist, ctx->nostore ? T * 2 * M : T * 2 * M * (size_t)(g.Ns + 1) * S));
         CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
         CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
         CKC(cudaMalloc(&ctx->tw, twb.size()));
@@ -863,6 +890,10 @@ scft_status scft_do_step(scft_ctx *ctx, int ii, const double *in, double *out, i
 {
     if (!ctx || !in || !out || ii < 0 || ii >= ctx->strn || s < 0 || s >= ctx->g.Ns)
         return SCFT_BAD_INPUT;
+    if (ctx->nostore) {
+        ctx->lasterr = "scft_do_step needs the full propagator store (context created with nostore)";
+        return SCFT_UNSUPPORTED;
+    }
     const size_t M = ctx->M;
     const size_t T = ctx->prec == SCFT_FP32 ? 4 : 8;
     const size_t slice = 2 * M;
@@ -897,6 +928,10 @@ scft_status scft_get_propagator(const scft_ctx *cctx, int ii, int which, int s, 
 {
     scft_ctx *ctx = const_cast<scft_ctx *>(cctx);
     if (!ctx || !outM || ii < 0 || ii >= ctx->nrep_alloc || s < 0 || s > ctx->g.Ns) return SCFT_BAD_INPUT;
+    if (ctx->nostore) {
+        ctx->lasterr = "scft_get_propagator needs the full propagator store (context created with nostore)";
+        return SCFT_UNSUPPORTED;
+    }
     const int slot = ctx->slot_of[ii];
     if (slot < 0) {
         ctx->lasterr = "propagators of this replica are no longer resident";
@@ -1438,6 +1473,7 @@ extern "C" {
 scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL)
 {
     if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    if (ctx->nostore) return scft_stress_ckpt(ctx, ii, ctx->ckK, dlnQ_dL, dF_dL, nullptr);
     const Geo &g = ctx->g;
     scft_status s = stress_alloc(ctx);
     if (s != SCFT_OK) return s;
@@ -1667,6 +1703,17 @@ scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, doub
 scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out)
 {
     if (!ctx || ii < 0 || ii >= ctx->strn || K < 1) return SCFT_BAD_INPUT;
+    return props_ckpt_impl(ctx, ii, K, lnQ_out, phis_out, bytes_out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// scft_props_ckpt for any replica slot of the context (the scratch replica of
+// scft_props_host included)
+scft_status props_ckpt_impl(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out)
+{
     const Geo &g = ctx->g;
     const int N = g.Ns, Nh = g.Nh, n1 = g.n1;
     const size_t M = g.M, T = ctx->prec == SCFT_FP32 ? 4 : 8;
@@ -1777,6 +1824,10 @@ scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, doubl
     return SCFT_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 // d lnQ/df of replica ii at its current fields with a continuous A fraction
 // (fcont): f moves the junction inside q's step n1 = floor(N f), whose field is
 // theta wA + (1-theta) wB with theta = N f - n1, so d/df = N d/dtheta and only
@@ -1786,6 +1837,10 @@ scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, doubl
 scft_status scft_dF_df(scft_ctx *ctx, int ii, double *dlnQ_df, double *dF_df)
 {
     if (!ctx || ii < 0 || ii >= ctx->strn) return SCFT_BAD_INPUT;
+    if (ctx->nostore) {
+        ctx->lasterr = "scft_dF_df needs the full propagator store (context created with nostore)";
+        return SCFT_UNSUPPORTED;
+    }
     const Geo &g = ctx->g;
     if (!g.jon) {
         ctx->lasterr = "scft_dF_df: needs a continuous A fraction (scft_problem.fcont = 1)";
@@ -2082,6 +2137,13 @@ scft_status scft_reset_stats(scft_ctx *ctx)
 scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms)
 {
     if (!ctx) return SCFT_BAD_INPUT;
+    if (ctx->nostore) {  // props run one replica at a time from checkpoints: nothing to schedule
+        if (groups_out) *groups_out = 1;
+        if (wide_out) *wide_out = ctx->L.ptile_wide;
+        if (times_ms)
+            for (int c = 0; c < 4; c++) times_ms[c] = -1;
+        return SCFT_OK;
+    }
     const scft_stats keep = ctx->stats;
     std::vector<int> all(ctx->strn);
     for (int i = 0; i < ctx->strn; i++) all[i] = i;

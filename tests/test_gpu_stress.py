@@ -207,3 +207,33 @@ def test_checkpointed_density_equals_props(built_lib, m, D, N, f, ens, K, prec, 
     if 3 <= K < N:
         assert nbytes < store + 6 * 8 * ctx.M
     print(m, N, K, prec, "checkpointed density bytes", nbytes, "full store", store)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_context_without_full_store(built_lib, precision):
+    """nostore: every props runs from checkpoints, so the W+ prelude and the
+    string iterations follow the full-store run (the same densities up to the
+    order of the FP64 sums); the box stress comes from the checkpointed
+    adjoint; the calls that read the store refuse."""
+    from scft_string_b200.configs import STRING_64, fields
+    c = dict(STRING_64, m=(16, 16, 16), D=(2.5, 2.5, 2.5), N=24, strn=4)
+    wm, wp = fields(c)
+    runs = []
+    for nostore in (0, 1):
+        ctx = S.StringSolver(dict(c, nostore=nostore, ckpt_K=5), precision=precision)
+        for ii in range(c["strn"]):
+            ctx.set_fields(ii, wm[ii], wp[ii])
+        ctx.solve_field0_all(50, 1e-6)
+        ctx.string_begin(100, 1e-3)
+        errs = [ctx.string_step()["errtot"] for _ in range(4)]
+        W = np.stack([ctx.get_fields(ii) for ii in range(c["strn"])])
+        st = ctx.stress(1)[1]
+        runs.append((errs, W, st, ctx))
+    (e0, W0, s0, _), (e1, W1, s1, ctx1) = runs
+    np.testing.assert_allclose(e1, e0, rtol=1e-9)
+    assert np.abs(W1 - W0).max() <= 1e-9 * np.abs(W0).max()
+    np.testing.assert_allclose(s1, s0, rtol=1e-7, atol=1e-12)
+    with pytest.raises(S.ScftError):
+        ctx1.do_step(0, np.ones(2 * ctx1.M), 0)
+    with pytest.raises(S.ScftError):
+        ctx1.propagator(0, 0, 1)

@@ -77,6 +77,8 @@ def lib():
         L.oc_props.restype = C.c_int
         L.oc_props.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp,
                                C.c_double, C.c_int]
+        L.oc_props_fcont.restype = C.c_int
+        L.oc_props_fcont.argtypes = L.oc_props.argtypes
         L.oc_density_q.restype = _dp
         L.oc_density_q.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oc_density_Q.argtypes = [C.c_void_p, _dp, _dp]
@@ -194,6 +196,17 @@ class Density:
         phis = np.zeros(6)
         rc = lib().oc_props(self.h, _p(w), C.byref(lnQ), int(Ns), float(alpha), float(phic),
                             _p(phis), float(f), int(ens))
+        if rc != 0:
+            raise ValueError("bad props arguments")
+        return lnQ.value, phis[:5].copy()
+
+    def props_fcont(self, w: np.ndarray, Ns, alpha, phic, f, ens):
+        """The continuous-f variant (f unrounded, junction step n1 = floor(Ns f))."""
+        assert w.size >= 6 * self.M
+        lnQ = C.c_double(0)
+        phis = np.zeros(6)
+        rc = lib().oc_props_fcont(self.h, _p(w), C.byref(lnQ), int(Ns), float(alpha), float(phic),
+                                  _p(phis), float(f), int(ens))
         if rc != 0:
             raise ValueError("bad props arguments")
         return lnQ.value, phis[:5].copy()

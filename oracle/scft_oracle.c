@@ -341,6 +341,7 @@ struct oc_density {
     double  *ksq;                /* Mk */
     double  *expKsq, *expKsq2;   /* Mk each */
     double  *E2p1, *Ep1, *E2m1, *Em1; /* M each: e^{-wA ds/4}, e^{-wA ds/2}, wB ... */
+    double  *E2j, *Ej;           /* M each: the junction step's tables (continuous f only) */
     double  *qs0, *qs1;          /* 2M each */
     double  *h;                  /* 2 fields * 2*Mk */
     double  *qq;                 /* 2*(Ns+1)*M: q(s) at 2sM, q^dagger(s) at (2s+1)M */
@@ -369,6 +370,8 @@ oc_density *oc_density_create(const int m[3], const double D[3], int Ns)
     d->Ep1 = d->E2p1 + M;
     d->E2m1 = d->E2p1 + 2 * M;
     d->Em1 = d->E2p1 + 3 * M;
+    d->E2j = (double *)malloc(sizeof(double) * 2 * M);
+    d->Ej = d->E2j + M;
     d->qs0 = (double *)malloc(sizeof(double) * 4 * M);
     d->qs1 = d->qs0 + 2 * M;
     d->h = (double *)malloc(sizeof(double) * 4 * Mk);
@@ -385,6 +388,7 @@ void oc_density_destroy(oc_density *d)
     free(d->expKsq);
     free(d->expKsq2);
     free(d->E2p1);
+    free(d->E2j);
     free(d->qs0);
     free(d->h);
     free(d->qq);
@@ -444,12 +448,22 @@ static void mult_k(oc_density *d, const double *K) /* Mult_self complex x real, 
     }
 }
 
-/* step::do_step, density.h:129-220 */
+/* step::do_step, density.h:129-220, with the tables of q (E2q, Eq) and of
+   q^dagger (E2d, Ed) for this step given */
+static void do_step_tables(oc_density *d, const double *in, double *out, const double *E2q, const double *Eq,
+                           const double *E2d, const double *Ed);
+
 void oc_do_step(oc_density *d, const double *in, double *out, int s, int n1, int n2)
 {
-    const int M = d->M;
     const double *E2q = (s < n1) ? d->E2p1 : d->E2m1, *Eq = (s < n1) ? d->Ep1 : d->Em1;
     const double *E2d = (s < n2) ? d->E2m1 : d->E2p1, *Ed = (s < n2) ? d->Em1 : d->Ep1;
+    do_step_tables(d, in, out, E2q, Eq, E2d, Ed);
+}
+
+static void do_step_tables(oc_density *d, const double *in, double *out, const double *E2q, const double *Eq,
+                           const double *E2d, const double *Ed)
+{
+    const int M = d->M;
     double *qs0 = d->qs0, *qs1 = d->qs1;
     /* first half step (Mult, GPU_kernels.h:192-196) */
 #pragma omp parallel for schedule(static)
@@ -501,12 +515,33 @@ double oc_reduction_sum(const double *a, int n)
     return cache[0];
 }
 
-/* density::props, density.h:344-459 */
+/* density::props, density.h:344-459.  fcont = 1 is the continuous-f variant
+   (no reference counterpart): n1 = floor(Ns f) whole A steps; q's step n1 and
+   q^dagger's step n2 - 1 see the field theta wA + (1 - theta) wB, theta = Ns f
+   - n1; theta of that step's trapezoid weight moves from the B block to the A
+   block of the Simpson sums.  At theta = 0 it is the reference
+   discretisation. */
+static int props_impl(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double phic,
+                      double *phis, double f, int ens, int fcont);
+
 int oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double phic,
              double *phis, double f, int ens)
 {
+    return props_impl(d, w, lnQ, Ns, alpha, phic, phis, f, ens, 0);
+}
+
+int oc_props_fcont(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double phic,
+                   double *phis, double f, int ens)
+{
+    return props_impl(d, w, lnQ, Ns, alpha, phic, phis, f, ens, 1);
+}
+
+static int props_impl(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double phic,
+                      double *phis, double f, int ens, int fcont)
+{
     const int M = d->M;
-    const int n1 = (int)round(Ns * f), n2 = Ns - n1, Nh = alpha * Ns;
+    const int n1 = fcont ? (int)floor(Ns * f) : (int)round(Ns * f), n2 = Ns - n1, Nh = alpha * Ns;
+    const double theta = fcont ? Ns * f - n1 : 0.0;
     const double ds = 1.0 / Ns;
     double Q1 = 0, Q2 = 0, QC = 0, zA = 0, zB = 0, zC = 0;
     double *c = d->cs;
@@ -516,12 +551,31 @@ int oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double
            *rhB = c + 9 * (size_t)M;
     if (ens != 1 && ens != 2) return -1;
     if (Ns > d->Ns || Nh > Ns || n1 < 0 || n1 > Ns) return -1;
+    if (fcont && (n1 >= Ns || Nh > n2 - 1)) return -1;
 
     oc_prepare_factors(d, ds, w);
+    if (fcont) {
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < M; r++) { /* theta wA + (1 - theta) wB = W+ + (2 theta - 1) W- */
+            d->E2j[r] = exp(-(w[r + M] + (2.0 * theta - 1.0) * w[r]) * ds / 4);
+            d->Ej[r] = d->E2j[r] * d->E2j[r];
+        }
+    }
     double *q0 = d->qq;
     for (int r = 0; r < 2 * M; r++) q0[r] = 1.0; /* Array_set_value, density.h:368-369 */
-    for (int s = 0; s < Ns; s++)
-        oc_do_step(d, d->qq + (size_t)2 * s * M, d->qq + (size_t)2 * (s + 1) * M, s, n1, n2);
+    for (int s = 0; s < Ns; s++) {
+        double *in = d->qq + (size_t)2 * s * M, *out = d->qq + (size_t)2 * (s + 1) * M;
+        if (!fcont) {
+            oc_do_step(d, in, out, s, n1, n2);
+            continue;
+        }
+        const int jq = (s == n1), jd = (s == n2 - 1);
+        const double *E2q = jq ? d->E2j : (s < n1) ? d->E2p1 : d->E2m1;
+        const double *Eq = jq ? d->Ej : (s < n1) ? d->Ep1 : d->Em1;
+        const double *E2d = jd ? d->E2j : (s < n2) ? d->E2m1 : d->E2p1;
+        const double *Ed = jd ? d->Ej : (s < n2) ? d->Em1 : d->Ep1;
+        do_step_tables(d, in, out, E2q, Eq, E2d, Ed);
+    }
 
 #define Q1S(s) (d->qq + (size_t)2 * (s) * M)
 #define Q2S(s) (d->qq + (size_t)(2 * (s) + 1) * M)
@@ -564,6 +618,11 @@ int oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha, double
         for (s = 1, wt = 4; s < n1; s++, wt = 6 - wt) rCA[r] += wt * Q1S(s)[r] * Q2S(Ns - s)[r];
         for (s = n1 + 1, wt = 4; s < Ns; s++, wt = 6 - wt)
             rCB[r] += wt * Q1S(s)[r] * Q2S(Ns - s)[r];
+        if (fcont) { /* theta of the junction step's trapezoid weight: B -> A */
+            const double tj = 1.5 * theta * (Q1S(n1)[r] * Q2S(Ns - n1)[r] + Q1S(n1 + 1)[r] * Q2S(Ns - n1 - 1)[r]);
+            rCA[r] += tj;
+            rCB[r] -= tj;
+        }
     }
     /* scale_concentrations (GPU_kernels.h:129-139) and sumconcs2 (GPU_kernels.h:114-127) */
 #pragma omp parallel for schedule(static)

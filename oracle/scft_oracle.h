@@ -65,6 +65,11 @@ void oc_do_step(oc_density *d, const double *in, double *out, int s, int n1, int
 int  oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
               double phic, double *phis, double f, int ens);
 /* Propagator slice access after oc_props: which=0 -> q(s), 1 -> q^dagger(s). */
+/* the continuous-f variant of oc_props (no reference counterpart; the
+   restatement of scft_problem.fcont): f is not rounded, the junction step
+   n1 = floor(Ns f) sees theta wA + (1 - theta) wB */
+int  oc_props_fcont(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
+                    double phic, double *phis, double f, int ens);
 const double *oc_density_q(const oc_density *d, int which, int s);
 /* Q2 = <q^dagger(Nh)>, QC = <q(Ns)> of the last props call. */
 void oc_density_Q(const oc_density *d, double *Q2, double *QC);

@@ -137,3 +137,26 @@ def test_gradients_entry_point(built_lib):
             assert df == ctx.dF_df(0)[1]
         else:
             assert np.isnan(df)
+
+
+@pytest.mark.parametrize("m,D,N,f,ens,prec,tol", [
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.47, 1, "fp64", 1e-11),
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.47, 2, "fp64", 1e-11),
+    ((32, 32, 32), (4.0, 4.0, 4.0), 24, 0.43, 1, "fp64", 1e-11),
+    ((32, 32, 32), (4.0, 4.0, 4.0), 24, 0.43, 1, "fp32", 5e-5),
+])
+def test_fcont_props_match_the_oracle(built_lib, m, D, N, f, ens, prec, tol):
+    """The CUDA continuous-f props against the oracle's FP64 restatement of the
+    same variant (oc_props_fcont): lnQ and the four density fields."""
+    import oracle as O
+    wm, wp = _fields(m, D, 8)
+    M = int(np.prod(m))
+    ctx = _ctx(m, D, N, f, ens, fcont=1, precision=prec)
+    conc, lnq, phis = _lnq(ctx, wm, wp)
+    od = O.Density(m, D, N)
+    w = np.zeros(6 * M)
+    w[:M], w[M:2 * M] = wm, wp
+    lnq0, phis0 = od.props_fcont(w, N, 0.1, 0.8, f, ens)
+    assert abs(lnq - lnq0) <= tol * max(1.0, abs(lnq0)), (lnq, lnq0)
+    assert np.abs(conc - w[2 * M:]).max() <= tol, np.abs(conc - w[2 * M:]).max()
+    np.testing.assert_allclose(phis, phis0, rtol=0, atol=tol)

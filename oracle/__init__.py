@@ -79,6 +79,8 @@ def lib():
                                C.c_double, C.c_int]
         L.oc_props_fcont.restype = C.c_int
         L.oc_props_fcont.argtypes = L.oc_props.argtypes
+        L.oc_stress.restype = C.c_int
+        L.oc_stress.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
         L.oc_density_q.restype = _dp
         L.oc_density_q.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oc_density_Q.argtypes = [C.c_void_p, _dp, _dp]
@@ -210,6 +212,15 @@ class Density:
         if rc != 0:
             raise ValueError("bad props arguments")
         return lnQ.value, phis[:5].copy()
+
+    def stress(self, W2M, Ns, alpha, phic, f, ens):
+        """d lnQ / d L_i (3 values) at the fields W2M = [W-, W+]."""
+        out = np.zeros(3)
+        rc = lib().oc_stress(self.h, _p(np.ascontiguousarray(W2M, np.float64)), int(Ns), float(alpha),
+                             float(phic), float(f), int(ens), _p(out))
+        if rc != 0:
+            raise ValueError("bad stress arguments")
+        return out
 
     def prepare(self, ds, W2M):
         lib().oc_prepare_factors(self.h, float(ds), _p(np.ascontiguousarray(W2M, np.float64)))

@@ -652,6 +652,97 @@ static int props_impl(oc_density *d, double *w, double *lnQ, int Ns, double alph
     return 0;
 }
 
+/* ================================================================ box stress
+   d lnQ / d L_i by the adjoint of the Richardson step, in real space: one
+   step is S = (4 E4 D2 E2 D2 E4 - E2 D1 E2)/3 (E4 = e^{-w ds/4}, E2 = E4^2,
+   D = FFT^-1 K FFT with K2 = e^{-k^2 ds/12}/M, K1 = e^{-k^2 ds/6}/M,
+   density.h:129-220), so
+     dS/dL_i x = 4/3 [E4 dD2_i(E2 D2 E4 x) + E4 D2(E2 dD2_i(E4 x))] - 1/3 E2 dD1_i(E2 x)
+   with dK/dL_i = K c 8 pi^2 n_i^2 / L_i^3, c = ds/12 (K2) or ds/6 (K1), and
+   dQC/dL = (1/M) sum_s <q^dagger(N-1-s), dS_s/dL q(s)>,
+   dQ2/dL = (1/M) sum_j <q^dagger(Nh-1-j), dS_B/dL q^dagger(j)> (q^dagger of a
+   step is the adjoint of q's mirrored step: S is symmetric).  A restatement
+   of the CUDA adjoint (no reference counterpart) that shares none of its
+   Fourier-space (Parseval) formulation. */
+static void apply_k(oc_density *d, const double *in, double *out, const double *K, int axis, double c)
+{
+    const oc_grid *g = d->g;
+    const int m0 = g->m[0], m1 = g->m[1], mk2 = g->mk2, Mk = d->Mk;
+    double *h = (double *)malloc(sizeof(double) * 2 * (size_t)Mk);
+    oc_fft_r2c(g, in, h);
+    for (int k = 0; k < Mk; k++) {
+        double v = K[k];
+        if (axis >= 0) {
+            const int K0 = k / (mk2 * m1), K1 = (k / mk2) % m1, k2 = k % mk2;
+            const int n = axis == 0 ? (K0 > m0 / 2 ? K0 - m0 : K0) : axis == 1 ? (K1 > m1 / 2 ? K1 - m1 : K1) : k2;
+            const double L = g->D[axis];
+            v *= c * 8.0 * PI * PI * (double)n * n / (L * L * L);
+        }
+        h[2 * k] *= v;
+        h[2 * k + 1] *= v;
+    }
+    oc_fft_c2r(g, h, out);
+    free(h);
+}
+
+/* <y, dS/dL_i x> for i = 0..2 with the step's tables E4, E2 */
+static void pair_stress(oc_density *d, const double *x, const double *y, const double *E4, const double *E2,
+                        double ds, double out[3])
+{
+    const int M = d->M;
+    double *a = (double *)calloc(6 * (size_t)M, sizeof(double));
+    double *b = a + M, *c = b + M, *t = c + M, *u = t + M, *v = u + M;
+    for (int r = 0; r < M; r++) a[r] = E4[r] * x[r];
+    apply_k(d, a, b, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) c[r] = E2[r] * b[r];
+    for (int i = 0; i < 3; i++) {
+        double acc = 0;
+        apply_k(d, c, t, d->expKsq2, i, ds / 12); /* E4 dD2 (E2 D2 E4 x) */
+        for (int r = 0; r < M; r++) acc += 4.0 / 3.0 * y[r] * E4[r] * t[r];
+        apply_k(d, a, t, d->expKsq2, i, ds / 12); /* E4 D2 (E2 dD2 (E4 x)) */
+        for (int r = 0; r < M; r++) u[r] = E2[r] * t[r];
+        apply_k(d, u, v, d->expKsq2, -1, 0);
+        for (int r = 0; r < M; r++) acc += 4.0 / 3.0 * y[r] * E4[r] * v[r];
+        for (int r = 0; r < M; r++) u[r] = E2[r] * x[r]; /* E2 dD1 (E2 x) */
+        apply_k(d, u, t, d->expKsq, i, ds / 6);
+        for (int r = 0; r < M; r++) acc -= 1.0 / 3.0 * y[r] * E2[r] * t[r];
+        out[i] = acc;
+    }
+    free(a);
+}
+
+int oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+              double dlnQ_dL[3])
+{
+    const int M = d->M;
+    const int n1 = (int)round(Ns * f), Nh = alpha * Ns;
+    const double ds = 1.0 / Ns;
+    double *w = (double *)calloc(6 * (size_t)M, sizeof(double));
+    memcpy(w, w2M, sizeof(double) * 2 * (size_t)M);
+    double lnQ, phis[5];
+    const int rc = props_impl(d, w, &lnQ, Ns, alpha, phic, phis, f, ens, 0);
+    free(w);
+    if (rc != 0) return rc;
+    double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0}, o[3];
+    for (int s = 0; s < Ns; s++) {
+        const int A = s < n1;
+        pair_stress(d, oc_density_q(d, 0, s), oc_density_q(d, 1, Ns - 1 - s), A ? d->E2p1 : d->E2m1,
+                    A ? d->Ep1 : d->Em1, ds, o);
+        for (int i = 0; i < 3; i++) dQC[i] += o[i];
+    }
+    for (int j = 0; j < Nh; j++) {
+        pair_stress(d, oc_density_q(d, 1, j), oc_density_q(d, 1, Nh - 1 - j), d->E2m1, d->Em1, ds, o);
+        for (int i = 0; i < 3; i++) dQ2[i] += o[i];
+    }
+    for (int i = 0; i < 3; i++) {
+        dQC[i] /= M;
+        dQ2[i] /= M;
+        dlnQ_dL[i] = ens == 1 ? phic * dQC[i] / d->QC + ((1.0 - phic) / alpha) * dQ2[i] / d->Q2
+                              : dQ2[i] + phic * dQC[i]; /* density.h:390, 398 */
+    }
+    return 0;
+}
+
 /* ================================================================ spline */
 /* cubefit_chunk_g, GPU_kernels.h:232-284, for one point */
 void oc_spline_coeffs(int strn, const double *x, const double *a_in, double *c, double *b,

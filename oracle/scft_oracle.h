@@ -70,6 +70,11 @@ int  oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
    n1 = floor(Ns f) sees theta wA + (1 - theta) wB */
 int  oc_props_fcont(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
                     double phic, double *phis, double f, int ens);
+/* d lnQ / d L_i of the fields w2M (W-, W+) by the adjoint of the Richardson
+   step applied in real space (no reference counterpart; the restatement of
+   scft_stress); runs oc_props first */
+int  oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f,
+               int ens, double dlnQ_dL[3]);
 const double *oc_density_q(const oc_density *d, int which, int s);
 /* Q2 = <q^dagger(Nh)>, QC = <q(Ns)> of the last props call. */
 void oc_density_Q(const oc_density *d, double *Q2, double *QC);

@@ -237,3 +237,29 @@ def test_context_without_full_store(built_lib, precision):
         ctx1.do_step(0, np.ones(2 * ctx1.M), 0)
     with pytest.raises(S.ScftError):
         ctx1.propagator(0, 0, 1)
+
+
+@pytest.mark.parametrize("m,D,N,ens", [((8, 12, 10), (2.0, 3.0, 2.5), 20, 1),
+                                        ((12, 8, 16), (3.1, 2.2, 4.0), 24, 2),
+                                        ((32, 32, 32), (4.0, 4.0, 4.0), 24, 1)])
+def test_adjoint_matches_the_oracle(built_lib, m, D, N, ens):
+    """The CUDA adjoint (Parseval sums of the FFT'd operands) against the
+    oracle's FP64 restatement (oc_stress: dS/dL applied in real space) at the
+    same fields: the full-store and the checkpointed FP64 adjoint to 1e-10,
+    the FP32 one within the FP32 bound of the finite-difference test."""
+    import oracle as O
+    D = np.array(D)
+    wm, wp = smooth_fields(m, D, 5)
+    f = round(N * 0.45) / N
+    ref = O.Density(m, D, N).stress(np.concatenate([wm, wp]), N, 0.1, 0.8, f, ens)
+    for prec in ("fp64", "fp32"):
+        ctx = S.Context(m, D, N, chi=12, f=0.45, phidb=0.8, ens=ens, alpha=0.1, strn=1, dostring=0,
+                        precision=prec)
+        ctx.set_fields(0, wm, wp)
+        full, _ = ctx.stress(0)
+        ck, _, _ = ctx.stress_ckpt(0, 5)
+        if prec == "fp64":
+            assert np.abs(full - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max()), (full, ref)
+            assert np.abs(ck - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max()), (ck, ref)
+        else:
+            assert np.allclose(full, ref, rtol=2e-4, atol=2e-6), (full, ref)

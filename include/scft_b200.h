@@ -170,6 +170,8 @@ scft_status scft_stress(scft_ctx *ctx, int ii, double *dlnQ_dL, double *dF_dL);
  * (two chain passes in all).  Device memory: *bytes_out (may be NULL) instead
  * of the (N+1) slice pairs of the full store; the context's full store is not
  * touched.  Same values as scft_stress up to the order of the FP64 sums. */
+scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL,
+                             double *bytes_out);
 /* d lnQ/df and dF/df = -d lnQ/df (exact at a converged saddle point) of
  * replica ii, for a context created with fcont = 1: the adjoint of the
  * junction step, whose field depends on f.  Either output may be NULL. */
@@ -186,8 +188,6 @@ scft_status scft_gradients(scft_ctx *ctx, int ii, double *dF_dL, double *dF_dchi
  * (may be NULL); the context's full store is not touched.  lnQ_out and
  * phis_out[5] as scft_get_conc (either may be NULL). */
 scft_status scft_props_ckpt(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out);
-scft_status scft_stress_ckpt(scft_ctx *ctx, int ii, int K, double *dlnQ_dL, double *dF_dL,
-                             double *bytes_out);
 /* Anderson-accelerated solution of replica ii's field equations (an option
  * beside the reference's simple mixing; no reference counterpart): residual
  * as scft.cu:605-607 without spring or string terms, history of nhist
@@ -233,7 +233,7 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
 scft_status scft_do_step_noalloc(const int *m, const double *D, int N, double f, const double *w2M,
                                  const double *in2M, double *out2M, int s, void *stream);
 
-/* ---- statistics ------------------------------------------------------- */
+/* ---- statistics (no reference counterpart) ---------------------------- */
 /* Records CUDA event `slot` (0..3) on the context's stream; elapsed device
  * time between two recorded slots (waits for the later one). */
 scft_status scft_timer_mark(scft_ctx *ctx, int slot);

@@ -81,6 +81,10 @@ def lib():
         L.oc_props_fcont.argtypes = L.oc_props.argtypes
         L.oc_stress.restype = C.c_int
         L.oc_stress.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+        L.oc_stress_fcont.restype = C.c_int
+        L.oc_stress_fcont.argtypes = L.oc_stress.argtypes
+        L.oc_dlnq_df.restype = C.c_int
+        L.oc_dlnq_df.argtypes = L.oc_stress.argtypes
         L.oc_density_q.restype = _dp
         L.oc_density_q.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oc_density_Q.argtypes = [C.c_void_p, _dp, _dp]
@@ -213,14 +217,25 @@ class Density:
             raise ValueError("bad props arguments")
         return lnQ.value, phis[:5].copy()
 
-    def stress(self, W2M, Ns, alpha, phic, f, ens):
-        """d lnQ / d L_i (3 values) at the fields W2M = [W-, W+]."""
+    def stress(self, W2M, Ns, alpha, phic, f, ens, fcont=False):
+        """d lnQ / d L_i (3 values) at the fields W2M = [W-, W+]; fcont selects
+        the continuous-f chain of props_fcont."""
         out = np.zeros(3)
-        rc = lib().oc_stress(self.h, _p(np.ascontiguousarray(W2M, np.float64)), int(Ns), float(alpha),
-                             float(phic), float(f), int(ens), _p(out))
+        fn = lib().oc_stress_fcont if fcont else lib().oc_stress
+        rc = fn(self.h, _p(np.ascontiguousarray(W2M, np.float64)), int(Ns), float(alpha),
+                float(phic), float(f), int(ens), _p(out))
         if rc != 0:
             raise ValueError("bad stress arguments")
         return out
+
+    def dlnq_df(self, W2M, Ns, alpha, phic, f, ens):
+        """d lnQ / df of the continuous-f variant at the fields W2M = [W-, W+]."""
+        out = np.zeros(1)
+        rc = lib().oc_dlnq_df(self.h, _p(np.ascontiguousarray(W2M, np.float64)), int(Ns), float(alpha),
+                              float(phic), float(f), int(ens), _p(out))
+        if rc != 0:
+            raise ValueError("bad dlnq_df arguments")
+        return float(out[0])
 
     def prepare(self, ds, W2M):
         lib().oc_prepare_factors(self.h, float(ds), _p(np.ascontiguousarray(W2M, np.float64)))

@@ -711,23 +711,32 @@ static void pair_stress(oc_density *d, const double *x, const double *y, const d
     free(a);
 }
 
-int oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
-              double dlnQ_dL[3])
+/* props of w2M (W-, W+) into the density's propagator store, fcont as props_impl */
+static int props_of(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+                    int fcont)
 {
     const int M = d->M;
-    const int n1 = (int)round(Ns * f), Nh = alpha * Ns;
-    const double ds = 1.0 / Ns;
     double *w = (double *)calloc(6 * (size_t)M, sizeof(double));
     memcpy(w, w2M, sizeof(double) * 2 * (size_t)M);
     double lnQ, phis[5];
-    const int rc = props_impl(d, w, &lnQ, Ns, alpha, phic, phis, f, ens, 0);
+    const int rc = props_impl(d, w, &lnQ, Ns, alpha, phic, phis, f, ens, fcont);
     free(w);
+    return rc;
+}
+
+static int stress_impl(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+                       int fcont, double dlnQ_dL[3])
+{
+    const int M = d->M;
+    const int n1 = fcont ? (int)floor(Ns * f) : (int)round(Ns * f), Nh = alpha * Ns;
+    const double ds = 1.0 / Ns;
+    const int rc = props_of(d, w2M, Ns, alpha, phic, f, ens, fcont);
     if (rc != 0) return rc;
     double dQC[3] = {0, 0, 0}, dQ2[3] = {0, 0, 0}, o[3];
     for (int s = 0; s < Ns; s++) {
-        const int A = s < n1;
-        pair_stress(d, oc_density_q(d, 0, s), oc_density_q(d, 1, Ns - 1 - s), A ? d->E2p1 : d->E2m1,
-                    A ? d->Ep1 : d->Em1, ds, o);
+        const int A = s < n1, J = fcont && s == n1;
+        pair_stress(d, oc_density_q(d, 0, s), oc_density_q(d, 1, Ns - 1 - s),
+                    J ? d->E2j : A ? d->E2p1 : d->E2m1, J ? d->Ej : A ? d->Ep1 : d->Em1, ds, o);
         for (int i = 0; i < 3; i++) dQC[i] += o[i];
     }
     for (int j = 0; j < Nh; j++) {
@@ -740,6 +749,67 @@ int oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phi
         dlnQ_dL[i] = ens == 1 ? phic * dQC[i] / d->QC + ((1.0 - phic) / alpha) * dQ2[i] / d->Q2
                               : dQ2[i] + phic * dQC[i]; /* density.h:390, 398 */
     }
+    return 0;
+}
+
+int oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+              double dlnQ_dL[3])
+{
+    return stress_impl(d, w2M, Ns, alpha, phic, f, ens, 0, dlnQ_dL);
+}
+
+int oc_stress_fcont(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+                    double dlnQ_dL[3])
+{
+    return stress_impl(d, w2M, Ns, alpha, phic, f, ens, 1, dlnQ_dL);
+}
+
+/* d lnQ/df of the continuous-f chain.  Only q's step n1 and q^dagger's step
+   n2 - 1 depend on f, through theta = Ns f - n1 in their field
+   wj = W+ + (2 theta - 1) W-, so with E4 = e^{-wj ds/4}, E2 = E4^2 and
+   g = dE4/dtheta / E4 = -(ds/2) W-:
+     dS/dtheta x = 4/3 [g E4 D2 E2 D2 E4 x + E4 D2 (2g E2) D2 E4 x + E4 D2 E2 D2 (g E4 x)]
+                 - 1/3 [2g E2 D1 E2 x + E2 D1 (2g E2 x)].
+   QC = <q(Ns)> sees it once, as <q^dagger(n2 - 1), dS/dtheta q(n1)> / M (S is
+   symmetric, so q^dagger carries the adjoint of q's later steps).  Q2 =
+   <q^dagger(Nh)> does not see it: Nh <= n2 - 1 puts q^dagger's junction step
+   after slice Nh. */
+int oc_dlnq_df(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f, int ens,
+               double *dlnQ_df)
+{
+    const int M = d->M;
+    const int n1 = (int)floor(Ns * f), n2 = Ns - n1;
+    const double ds = 1.0 / Ns;
+    const int rc = props_of(d, w2M, Ns, alpha, phic, f, ens, 1);
+    if (rc != 0) return rc;
+    const double *x = oc_density_q(d, 0, n1), *y = oc_density_q(d, 1, n2 - 1);
+    const double *E4 = d->E2j, *E2 = d->Ej;
+    double *g = (double *)calloc(5 * (size_t)M, sizeof(double));
+    double *a = g + M, *b = a + M, *c = b + M, *e = c + M;
+    for (int r = 0; r < M; r++) g[r] = -0.5 * ds * w2M[r];
+    double t = 0;
+    for (int r = 0; r < M; r++) a[r] = E4[r] * x[r]; /* first half-step pair: E4 D2 E2 D2 E4 x */
+    apply_k(d, a, b, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) c[r] = E2[r] * b[r];
+    apply_k(d, c, e, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) t += 4.0 / 3.0 * y[r] * g[r] * E4[r] * e[r];
+    for (int r = 0; r < M; r++) c[r] = 2.0 * g[r] * E2[r] * b[r];
+    apply_k(d, c, e, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) t += 4.0 / 3.0 * y[r] * E4[r] * e[r];
+    for (int r = 0; r < M; r++) a[r] = g[r] * E4[r] * x[r];
+    apply_k(d, a, b, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) c[r] = E2[r] * b[r];
+    apply_k(d, c, e, d->expKsq2, -1, 0);
+    for (int r = 0; r < M; r++) t += 4.0 / 3.0 * y[r] * E4[r] * e[r];
+    for (int r = 0; r < M; r++) a[r] = E2[r] * x[r]; /* full step: E2 D1 E2 x */
+    apply_k(d, a, b, d->expKsq, -1, 0);
+    for (int r = 0; r < M; r++) t -= 1.0 / 3.0 * y[r] * 2.0 * g[r] * E2[r] * b[r];
+    for (int r = 0; r < M; r++) a[r] = 2.0 * g[r] * E2[r] * x[r];
+    apply_k(d, a, b, d->expKsq, -1, 0);
+    for (int r = 0; r < M; r++) t -= 1.0 / 3.0 * y[r] * E2[r] * b[r];
+    free(g);
+    const double dQC = t / M;
+    *dlnQ_df = Ns * (ens == 1 ? phic * dQC / d->QC : phic * dQC); /* density.h:390, 398 */
     return 0;
 }
 

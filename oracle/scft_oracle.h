@@ -64,7 +64,6 @@ void oc_do_step(oc_density *d, const double *in, double *out, int s, int n1, int
  * Returns 0, or -1 for an ens outside {1,2}. */
 int  oc_props(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
               double phic, double *phis, double f, int ens);
-/* Propagator slice access after oc_props: which=0 -> q(s), 1 -> q^dagger(s). */
 /* the continuous-f variant of oc_props (no reference counterpart; the
    restatement of scft_problem.fcont): f is not rounded, the junction step
    n1 = floor(Ns f) sees theta wA + (1 - theta) wB */
@@ -75,6 +74,17 @@ int  oc_props_fcont(oc_density *d, double *w, double *lnQ, int Ns, double alpha,
    scft_stress); runs oc_props first */
 int  oc_stress(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f,
                int ens, double dlnQ_dL[3]);
+/* oc_stress for the continuous-f variant: the chain of oc_props_fcont, with
+   the junction step's tables at q's step n1 */
+int  oc_stress_fcont(oc_density *d, const double *w2M, int Ns, double alpha, double phic,
+                     double f, int ens, double dlnQ_dL[3]);
+/* d lnQ / df of the continuous-f variant (the restatement of scft_dF_df):
+   Ns times the derivative of lnQ in the junction step's theta, with
+   dS/dtheta applied in real space; runs oc_props_fcont first.  Returns -1
+   where oc_props_fcont does. */
+int  oc_dlnq_df(oc_density *d, const double *w2M, int Ns, double alpha, double phic, double f,
+                int ens, double *dlnQ_df);
+/* Propagator slice access after oc_props: which=0 -> q(s), 1 -> q^dagger(s). */
 const double *oc_density_q(const oc_density *d, int which, int s);
 /* Q2 = <q^dagger(Nh)>, QC = <q(Ns)> of the last props call. */
 void oc_density_Q(const oc_density *d, double *Q2, double *QC);

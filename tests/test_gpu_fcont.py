@@ -160,3 +160,29 @@ def test_fcont_props_match_the_oracle(built_lib, m, D, N, f, ens, prec, tol):
     assert abs(lnq - lnq0) <= tol * max(1.0, abs(lnq0)), (lnq, lnq0)
     assert np.abs(conc - w[2 * M:]).max() <= tol, np.abs(conc - w[2 * M:]).max()
     np.testing.assert_allclose(phis, phis0, rtol=0, atol=tol)
+
+
+@pytest.mark.parametrize("m,D,N,f,ens", [
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.47, 1),
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.47, 2),
+    ((8, 12, 10), (2.0, 3.0, 2.5), 20, 0.512, 2),
+    ((32, 32, 32), (4.0, 4.0, 4.0), 24, 0.43, 1),
+])
+def test_fcont_derivatives_match_the_oracle(built_lib, m, D, N, f, ens):
+    """The CUDA d lnQ/df (junction adjoint, Parseval form) and box stress
+    with the junction step against the oracle's FP64 restatements
+    (oc_dlnq_df, oc_stress_fcont: dS/dtheta and dS/dL applied in real space),
+    at the same fields, FP64."""
+    import oracle as O
+    wm, wp = _fields(m, D, 9)
+    ctx = _ctx(m, D, N, f, ens)
+    ctx.set_fields(0, wm, wp)
+    dlnq, _ = ctx.dF_df(0)
+    dl, _ = ctx.stress(0)
+    od = O.Density(m, D, N)
+    W = np.concatenate([wm, wp])
+    dlnq0 = od.dlnq_df(W, N, 0.1, 0.8, f, ens)
+    dl0 = od.stress(W, N, 0.1, 0.8, f, ens, fcont=True)
+    print("d lnQ/df", dlnq, dlnq0, "stress", dl, dl0)
+    assert abs(dlnq - dlnq0) <= 1e-9 * max(1.0, abs(dlnq0)), (dlnq, dlnq0)
+    np.testing.assert_allclose(dl, dl0, rtol=1e-9, atol=1e-12)

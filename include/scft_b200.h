@@ -242,11 +242,19 @@ scft_status scft_get_stats(const scft_ctx *ctx, scft_stats *st);
 scft_status scft_reset_stats(scft_ctx *ctx);
 
 /* Binary FP64 checkpoint (no reference counterpart; the ASCII win files stay
- * the drop-in format): problem record with the current box and the fields of
- * every replica, with a hash of the field bytes.  Loading checks the grid and
- * replica count against the context and the hash, then sets box and fields. */
+ * the drop-in format): problem record with the current box, the fields and
+ * the box of every replica, and a hash of the field and box bytes.  Loading
+ * checks the grid and replica count against the context and the hash, then
+ * sets boxes and fields.  Files of earlier versions and of shorter (older) or
+ * longer problem records load too: the record only grows at its end. */
 scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path);
 scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path);
+/* The header of a checkpoint file, checked as scft_load_checkpoint checks the
+ * file (hash included) but with no context and no device: format version,
+ * replica count, m[3] and the common box D[3].  Any output may be NULL;
+ * BAD_INPUT for a file that cannot be opened or that a load would refuse for
+ * its content. */
+scft_status scft_checkpoint_info(const char *path, int *version, int *strn, int *m, double *D);
 /* Picks the schedule of a props round by timing rounds of all replicas at
  * their current fields: 1 or 2 concurrent slot groups, and x-pencil tiles of
  * the default or twice the width (grids with tensor-map pencils only).  The

@@ -80,7 +80,7 @@ EXPORTS = [
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
     "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
-    "scft_gradients", "scft_props_ckpt",
+    "scft_gradients", "scft_props_ckpt", "scft_checkpoint_info",
 ]
 
 _lib = None
@@ -145,6 +145,7 @@ def lib():
     L.scft_props_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_get_box_replica.argtypes = [vp, C.c_int, _dp]
     L.scft_load_checkpoint.argtypes = [vp, C.c_char_p]
+    L.scft_checkpoint_info.argtypes = [C.c_char_p, _ip, _ip, _ip, _dp]
     _lib = L
     return L
 
@@ -443,6 +444,19 @@ class Density:
 
     def props(self, w, Ns, alpha, phic, f):
         return self.ctx.props_host(w, Ns, alpha, phic, f)
+
+
+def checkpoint_info(path) -> dict:
+    """Header of a checkpoint file (version, replica count, grid, common box),
+    checked as a load checks it; needs no device.  Raises ScftError for a file
+    that a load would refuse."""
+    v, n = C.c_int(0), C.c_int(0)
+    m = (C.c_int * 3)()
+    D = np.zeros(3)
+    rc = lib().scft_checkpoint_info(os.fsencode(path), C.byref(v), C.byref(n), m, _p(D))
+    if rc != 0:
+        raise ScftError(rc, f"scft_checkpoint_info: {lib().scft_status_string(rc).decode()}: {path}")
+    return {"version": v.value, "strn": n.value, "m": (m[0], m[1], m[2]), "D": tuple(float(x) for x in D)}
 
 
 def StringSolver(cfg: dict, precision="fp64", batched=True, springsteps=0, device=0) -> Context:

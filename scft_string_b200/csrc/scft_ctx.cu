@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <cstdlib>
 #include <cmath>
@@ -1305,7 +1306,13 @@ scft_status upload_box(scft_ctx *ctx, int r, const double *D)
     return SCFT_OK;
 }
 
-bool box_ok(const double *D) { return D && D[0] > 0 && D[1] > 0 && D[2] > 0; }
+bool box_ok(const double *D)
+{
+    if (!D) return false;
+    for (int i = 0; i < 3; i++)
+        if (!(std::isfinite(D[i]) && D[i] > 0)) return false;
+    return true;
+}
 }  // namespace
 
 // the box of every replica (and the scratch replica of scft_props_host)
@@ -1313,6 +1320,7 @@ scft_status scft_set_box(scft_ctx *ctx, const double *D)
 {
     if (!ctx || !box_ok(D)) return SCFT_BAD_INPUT;
     for (int i = 0; i < 3; i++) ctx->p.D[i] = D[i];
+    std::fill(ctx->slot_of.begin(), ctx->slot_of.end(), -1);  // stored propagators are of the old box
     for (int r = 0; r < ctx->nrep_alloc; r++) {
         scft_status s = upload_box(ctx, r, D);
         if (s != SCFT_OK) return s;
@@ -2191,12 +2199,17 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
 
 // ---- binary FP64 checkpoint (no reference counterpart: the reference keeps
 // only the ASCII win files, scft.cu:785-788).  Layout, host byte order:
-//   "SCFTCKP1" | u32 version (2) | u32 sizeof(scft_problem) | scft_problem
-//   (with the last common box) | i32 strn | i64 M | strn x 2M doubles
-//   (W-, W+) | strn x 3 doubles (each replica's box) | u64 FNV-1a hash of the
-//   field and box bytes.  Version 1 files (no per-replica boxes) load too.
+//   "SCFTCKP1" | u32 version (2) | u32 P = sizeof(scft_problem) | P bytes of
+//   scft_problem (with the last common box) | i32 strn | i64 M | strn x 2M
+//   doubles (W-, W+) | strn x 3 doubles (each replica's box) | u64 FNV-1a hash
+//   of the field and box bytes.  Version 1 has no per-replica boxes.
+// scft_problem only ever grows at its end, so the reader takes a problem block
+// of any size that covers m and D: fields missing from a shorter (older)
+// block read as 0, their defaults, and the tail of a longer one is skipped.
 namespace {
 constexpr char kCkptMagic[8] = {'S', 'C', 'F', 'T', 'C', 'K', 'P', '1'};
+constexpr uint64_t kFnvBasis = 1469598103934665603ull;
+constexpr uint32_t kMaxProblemBytes = 1u << 16;
 
 uint64_t fnv1a(uint64_t h, const void *data, size_t n)
 {
@@ -2206,6 +2219,69 @@ uint64_t fnv1a(uint64_t h, const void *data, size_t n)
         h *= 1099511628211ull;
     }
     return h;
+}
+
+struct CkptFile {
+    uint32_t version = 0;
+    scft_problem p;
+    int32_t strn = 0;
+    int64_t M = 0;
+    std::vector<double> fields, boxes;  // fields only when asked for
+};
+
+// reads and checks a checkpoint file; on failure returns false with `why`
+bool read_checkpoint(const char *path, bool keep_fields, CkptFile &c, std::string &why)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        why = std::string("cannot open ") + path;
+        return false;
+    }
+    auto fail = [&](const char *w) {
+        fclose(f);
+        why = w;
+        return false;
+    };
+    char magic[8];
+    uint32_t psz = 0;
+    std::memset(&c.p, 0, sizeof(c.p));
+    if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return fail("not a checkpoint");
+    if (fread(&c.version, 4, 1, f) != 1 || (c.version != 1 && c.version != 2) || fread(&psz, 4, 1, f) != 1)
+        return fail("unsupported version");
+    if (psz < offsetof(scft_problem, N) || psz > kMaxProblemBytes) return fail("unsupported problem block");
+    const size_t take = std::min<size_t>(psz, sizeof(scft_problem));
+    if (fread(&c.p, take, 1, f) != 1) return fail("truncated header");
+    if (psz > take && fseek(f, (long)(psz - take), SEEK_CUR) != 0) return fail("truncated header");
+    if (fread(&c.strn, 4, 1, f) != 1 || fread(&c.M, 8, 1, f) != 1) return fail("truncated header");
+    const int64_t Mg = (int64_t)c.p.m[0] * c.p.m[1] * c.p.m[2];
+    if (c.strn < 1 || c.p.m[0] < 1 || c.p.m[1] < 1 || c.p.m[2] < 1 || c.M != Mg) return fail("inconsistent header");
+    const size_t nf = 2 * (size_t)c.M * (size_t)c.strn;
+    uint64_t hh = kFnvBasis;
+    if (keep_fields) {
+        c.fields.resize(nf);
+        if (fread(c.fields.data(), sizeof(double), nf, f) != nf) return fail("truncated fields");
+        hh = fnv1a(hh, c.fields.data(), nf * sizeof(double));
+    } else {
+        std::vector<double> chunk(1 << 17);
+        for (size_t done = 0; done < nf;) {
+            const size_t n = std::min(chunk.size(), nf - done);
+            if (fread(chunk.data(), sizeof(double), n, f) != n) return fail("truncated fields");
+            hh = fnv1a(hh, chunk.data(), n * sizeof(double));
+            done += n;
+        }
+    }
+    c.boxes.clear();
+    if (c.version == 2) {
+        c.boxes.resize(3 * (size_t)c.strn);
+        if (fread(c.boxes.data(), sizeof(double), c.boxes.size(), f) != c.boxes.size())
+            return fail("truncated boxes");
+        hh = fnv1a(hh, c.boxes.data(), c.boxes.size() * sizeof(double));
+    }
+    uint64_t h = 0;
+    if (fread(&h, 8, 1, f) != 1) return fail("truncated hash");
+    if (h != hh) return fail("hash mismatch");
+    fclose(f);
+    return true;
 }
 }  // namespace
 
@@ -2224,7 +2300,7 @@ scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path)
     bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(&ver, 4, 1, f) == 1 && fwrite(&psz, 4, 1, f) == 1 &&
               fwrite(&ctx->p, psz, 1, f) == 1 && fwrite(&strn, 4, 1, f) == 1 && fwrite(&M, 8, 1, f) == 1;
     std::vector<double> w(2 * (size_t)M);
-    uint64_t h = 1469598103934665603ull;
+    uint64_t h = kFnvBasis;
     for (int ii = 0; ok && ii < ctx->strn; ii++) {
         scft_status s = scft_get_fields(ctx, ii, w.data());
         if (s != SCFT_OK) {
@@ -2251,51 +2327,43 @@ scft_status scft_save_checkpoint(scft_ctx *ctx, const char *path)
 scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path)
 {
     if (!ctx || !path) return SCFT_BAD_INPUT;
-    FILE *f = fopen(path, "rb");
-    if (!f) {
-        ctx->lasterr = std::string("scft_load_checkpoint: cannot open ") + path;
+    CkptFile c;
+    std::string why;
+    if (!read_checkpoint(path, true, c, why)) {
+        ctx->lasterr = "scft_load_checkpoint: " + why;
         return SCFT_BAD_INPUT;
     }
-    auto fail = [&](const char *why) {
-        fclose(f);
-        ctx->lasterr = std::string("scft_load_checkpoint: ") + why;
+    if (c.strn != ctx->strn || c.M != (int64_t)ctx->M || c.p.m[0] != ctx->p.m[0] || c.p.m[1] != ctx->p.m[1] ||
+        c.p.m[2] != ctx->p.m[2]) {
+        ctx->lasterr = "scft_load_checkpoint: grid or replica count differs from the context";
         return SCFT_BAD_INPUT;
-    };
-    char magic[8];
-    uint32_t ver = 0, psz = 0;
-    scft_problem p;
-    int32_t strn = 0;
-    int64_t M = 0;
-    if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return fail("not a checkpoint");
-    if (fread(&ver, 4, 1, f) != 1 || (ver != 1 && ver != 2) || fread(&psz, 4, 1, f) != 1 ||
-        psz != sizeof(scft_problem))
-        return fail("unsupported version");
-    if (fread(&p, psz, 1, f) != 1 || fread(&strn, 4, 1, f) != 1 || fread(&M, 8, 1, f) != 1)
-        return fail("truncated header");
-    if (strn != ctx->strn || M != ctx->M || p.m[0] != ctx->p.m[0] || p.m[1] != ctx->p.m[1] ||
-        p.m[2] != ctx->p.m[2])
-        return fail("grid or replica count differs from the context");
-    std::vector<double> all(2 * (size_t)M * strn), boxes;
-    if (fread(all.data(), sizeof(double), all.size(), f) != all.size()) return fail("truncated fields");
-    uint64_t hh = fnv1a(1469598103934665603ull, all.data(), all.size() * sizeof(double));
-    if (ver == 2) {
-        boxes.resize(3 * (size_t)strn);
-        if (fread(boxes.data(), sizeof(double), boxes.size(), f) != boxes.size()) return fail("truncated boxes");
-        hh = fnv1a(hh, boxes.data(), boxes.size() * sizeof(double));
     }
-    uint64_t h = 0;
-    if (fread(&h, 8, 1, f) != 1) return fail("truncated hash");
-    if (h != hh) return fail("hash mismatch");
-    fclose(f);
-    scft_status s = scft_set_box(ctx, p.D);
+    scft_status s = scft_set_box(ctx, c.p.D);
     if (s != SCFT_OK) return s;
-    for (int ii = 0; ii < (int)boxes.size() / 3; ii++) {
-        s = scft_set_box_replica(ctx, ii, &boxes[3 * (size_t)ii]);
+    for (int ii = 0; ii < (int)c.boxes.size() / 3; ii++) {
+        s = scft_set_box_replica(ctx, ii, &c.boxes[3 * (size_t)ii]);
         if (s != SCFT_OK) return s;
     }
-    for (int ii = 0; ii < strn; ii++) {
-        s = scft_set_fields(ctx, ii, all.data() + (size_t)ii * 2 * M);
+    for (int ii = 0; ii < c.strn; ii++) {
+        s = scft_set_fields(ctx, ii, c.fields.data() + (size_t)ii * 2 * c.M);
         if (s != SCFT_OK) return s;
+    }
+    return SCFT_OK;
+}
+
+// header of a checkpoint file, checked as scft_load_checkpoint checks it (hash
+// included), with no context and no device
+scft_status scft_checkpoint_info(const char *path, int *version, int *strn, int *m, double *D)
+{
+    if (!path) return SCFT_BAD_INPUT;
+    CkptFile c;
+    std::string why;
+    if (!read_checkpoint(path, false, c, why)) return SCFT_BAD_INPUT;
+    if (version) *version = (int)c.version;
+    if (strn) *strn = c.strn;
+    for (int i = 0; i < 3; i++) {
+        if (m) m[i] = c.p.m[i];
+        if (D) D[i] = c.p.D[i];
     }
     return SCFT_OK;
 }

@@ -290,6 +290,25 @@ int main(int argc, char *argv[])
     p.batched = batched;
     p.device = 0;
     p.fcont = fcont;
+    if (const char *dry = std::getenv("SCFT_DRY_RUN"); dry && dry[0] == '1') {
+        // the resolved input and the start fields, then exit before any device
+        // call: the input handling checked without a GPU
+        printf("dryrun problem m=%d %d %d D=%.17g %.17g %.17g N=%d alpha=%.17g ens=%d phidb=%.17g chi=%.17g "
+               "f=%.17g strn=%d fix=%d %d dostring=%d springsteps=%d precision=%d batched=%d fcont=%d\n",
+               m[0], m[1], m[2], D[0], D[1], D[2], N, alpha, ens, phidb, chi, f, strn, fix[0], fix[1], dostring,
+               springsteps, precision, batched, fcont);
+        printf("dryrun run readwin=%d justFE=%d nsterp=%d errtol=%.17g checkpoint=%d restart=%d\n", readwin, justFE,
+               nsterp, errtol_stop, checkpoint, restart);
+        for (int ii = 0; ii < strn; ii++) {
+            double sm = 0, sp = 0;
+            for (long r = 0; r < M; r++) {
+                sm += W[ii][r];
+                sp += W[ii][r + M];
+            }
+            printf("dryrun field %d %.17g %.17g %.17g %.17g\n", ii, W[ii][0], W[ii][M], sm, sp);
+        }
+        return 0;
+    }
     CHECK(scft_create(&p, &ctx));
     for (int ii = 0; ii < strn; ii++) CHECK(scft_set_fields(ctx, ii, W[ii].data()));
     if (restart == 1 && fexist("fields.ckpt")) {

@@ -15,6 +15,8 @@
 //   restart   1: start from `fields.ckpt` (box and fields) instead of win files
 //   fcont     1: continuous A fraction (no rounding of f; junction step inside
 //             the chain), 0 (default): the reference's rounded f
+// Environment: SCFT_DRY_RUN=1 prints the resolved input and the start fields
+// and exits before any device call.
 #include <csignal>
 #include <cmath>
 #include <cstdio>

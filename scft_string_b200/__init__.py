@@ -193,6 +193,7 @@ class Context:
         self.h = h
 
     def close(self):
+        """Destroys the context (scft_destroy; the reference's `delete D2`)."""
         if getattr(self, "h", None):
             lib().scft_destroy(self.h)
             self.h = None
@@ -207,6 +208,8 @@ class Context:
 
     # fields --------------------------------------------------------------
     def set_fields(self, ii, wm, wp):
+        """Replica ii's W- and W+ (M each): the first 2M entries of the reference's
+        W[ii] (scft.cu:1037-1051, 1062)."""
         w = np.ascontiguousarray(np.concatenate([np.ravel(wm), np.ravel(wp)]), np.float64)
         self._ck(lib().scft_set_fields(self.h, int(ii), _p(w)))
 
@@ -221,6 +224,9 @@ class Context:
         self._ck(lib().scft_set_fields(self.h, int(ii), _p(w2m)))
 
     def get_conc(self, ii):
+        """(concentrations [phiA, phiB, phih, phicB] as 4M doubles, lnQ, phis[5]) of
+        replica ii's last props: W[ii][2M:6M), lnQ and phis of density::props
+        (density.h:344-459)."""
         c = np.zeros(4 * self.M)
         lnQ = C.c_double()
         phis = np.zeros(5)
@@ -228,12 +234,16 @@ class Context:
         return c, lnQ.value, phis
 
     def doiis(self):
+        """Replica ownership mask of the single process (scft.cu:953-975): 1 for
+        every replica, 0 for the fixed ends when fix is set (scft.cu:587-588)."""
         d = np.zeros(self.strn, np.int32)
         self._ck(lib().scft_get_doiis(self.h, d.ctypes.data_as(_ip)))
         return d
 
     # density -------------------------------------------------------------
     def props(self, ii):
+        """density::props (density.h:344-459) of replica ii on its device-resident
+        fields; results via get_conc(ii)."""
         self._ck(lib().scft_props(self.h, int(ii)))
 
     def props_host(self, w, Ns, alpha, phic, f, ii=0):
@@ -245,29 +255,41 @@ class Context:
         return lnQ.value, phis
 
     def do_step(self, ii, qin, s):
+        """One Richardson contour step (step::do_step, density.h:129-220) of the
+        slice qin = [q(s), q^dagger(s)] (2M doubles) in replica ii's fields;
+        returns [q(s+1), q^dagger(s+1)]."""
         qin = np.ascontiguousarray(qin, np.float64).reshape(-1)
         out = np.zeros(2 * self.M)
         self._ck(lib().scft_do_step(self.h, int(ii), _p(qin), _p(out), int(s)))
         return out
 
     def propagator(self, ii, which, s):
+        """Slice s of replica ii's last props: which 0 = q(s), 1 = q^dagger(s)
+        (the reference's dev_qq, density.h:368-385)."""
         out = np.zeros(self.M)
         self._ck(lib().scft_get_propagator(self.h, int(ii), int(which), int(s), _p(out)))
         return out
 
     # solvers -------------------------------------------------------------
     def solve_field0(self, ii, maxIter, errTol):
+        """W+ relaxation of replica ii (solve_field0, scft.cu:516-554); returns
+        the reference's final k."""
         k = C.c_int()
         self._ck(lib().scft_solve_field0(self.h, int(ii), int(maxIter), float(errTol), C.byref(k)))
         return k.value
 
     def solve_field0_all(self, maxIter=5000, errTol=1e-4):
+        """W+ relaxation of every replica, the prelude of main (scft.cu:1105);
+        returns k per replica."""
         k = np.zeros(self.strn, np.int32)
         self._ck(lib().scft_solve_field0_all(self.h, int(maxIter), float(errTol),
                                              k.ctypes.data_as(_ip)))
         return k
 
     def solve_field(self, maxIter, errTol=1e-3, doii=-1):
+        """solve_field (scft.cu:559-809), doii = -1 for the whole string; returns
+        (iterations run, per-iteration records, errs and errs3 per iteration and
+        replica)."""
         n = max(1, int(maxIter))
         reps = (IterReport * n)()
         errs = np.zeros(n * self.strn)
@@ -282,9 +304,12 @@ class Context:
             errs3[: k * self.strn].reshape(k, self.strn)
 
     def string_begin(self, maxIter, errTol=1e-3, doii=-1):
+        """Starts solve_field one iteration at a time (see string_step)."""
         self._ck(lib().scft_string_begin(self.h, int(doii), int(maxIter), float(errTol)))
 
     def string_step(self):
+        """One iteration of the solve_field loop (scft.cu:592-806): its record,
+        errs, errs3 and whether the loop would stop."""
         rep = IterReport()
         errs = np.zeros(self.strn)
         errs3 = np.zeros(self.strn)
@@ -295,11 +320,14 @@ class Context:
                     done=bool(done.value))
 
     def string_end(self):
+        """Ends the iteration-at-a-time solve; returns the reference's final k."""
         k = C.c_int()
         self._ck(lib().scft_string_end(self.h, C.byref(k)))
         return k.value
 
     def free_energy(self):
+        """FreeE (scft.cu:812-853): total FE and, per replica, FEs, FEs0, FEs1,
+        phctot and the arc-length coordinate alf."""
         s = self.strn
         FE = C.c_double()
         FEs, F0, F1, ph, alf = (np.zeros(s) for _ in range(5))
@@ -308,6 +336,9 @@ class Context:
         return dict(FE=FE.value, FEs=FEs, FEs0=F0, FEs1=F1, phctot=ph, alf=alf)
 
     def spline_derivs(self, x, Wm, doiis):
+        """density::splineDerivsChunked (density.h:491-508) over the whole grid:
+        dW-/dalpha of every replica at its knot x[ii] (rows of Wm: W- per
+        replica)."""
         strn, M = Wm.shape
         Wm = np.ascontiguousarray(Wm, np.float64)
         out = np.zeros((strn, M))
@@ -318,6 +349,9 @@ class Context:
         return out
 
     def spline_redist(self, x, xref, Wm, doiis, lam):
+        """density::splineRedistChunked (density.h:511-528) over the whole grid:
+        returns a copy of Wm with interior replicas (doiis == 1) relaxed by lam
+        towards the spline at xref."""
         strn, M = Wm.shape
         Wm = np.ascontiguousarray(Wm, np.float64).copy()
         d = np.ascontiguousarray(doiis, np.int32)
@@ -328,12 +362,15 @@ class Context:
         return Wm
 
     def stats(self):
+        """Counters of the context: props calls, contour steps, kernel launches
+        and device seconds in props rounds (no reference counterpart)."""
         st = Stats()
         self._ck(lib().scft_get_stats(self.h, C.byref(st)))
         return dict(props_calls=st.props_calls, contour_steps=st.contour_steps,
                     kernel_launches=st.kernel_launches, props_seconds=st.props_seconds)
 
     def reset_stats(self):
+        """Zeroes the counters of stats()."""
         self._ck(lib().scft_reset_stats(self.h))
 
     def set_box(self, D, ii=None):
@@ -345,6 +382,8 @@ class Context:
             self._ck(lib().scft_set_box_replica(self.h, int(ii), _p(D)))
 
     def get_box(self, ii=None):
+        """Box lengths D[3] of the context, or of replica ii (the reference's D,
+        default 4 4 4 at scft.cu:917)."""
         D = np.zeros(3)
         if ii is None:
             self._ck(lib().scft_get_box(self.h, _p(D)))
@@ -404,6 +443,8 @@ class Context:
         return dL, dchi.value, df.value
 
     def dF_dchi(self, ii=0):
+        """dF/d(chi N) of replica ii at a converged saddle point:
+        1/4 - <W-^2>/chi^2 (no reference counterpart)."""
         v = C.c_double()
         self._ck(lib().scft_dF_dchi(self.h, int(ii), C.byref(v)))
         return v.value
@@ -421,6 +462,8 @@ class Context:
         self._ck(lib().scft_save_checkpoint(self.h, os.fsencode(path)))
 
     def load_checkpoint(self, path):
+        """Boxes and fields of every replica from a binary checkpoint (hash,
+        grid and replica count checked)."""
         self._ck(lib().scft_load_checkpoint(self.h, os.fsencode(path)))
 
     def timer_mark(self, slot):
@@ -428,6 +471,7 @@ class Context:
         self._ck(lib().scft_timer_mark(self.h, int(slot)))
 
     def timer_elapsed_ms(self, a, b):
+        """Device milliseconds between timer slots a and b (waits for b)."""
         ms = C.c_double()
         self._ck(lib().scft_timer_elapsed(self.h, int(a), int(b), C.byref(ms)))
         return ms.value
@@ -443,6 +487,8 @@ class Density:
         self.M = self.ctx.M
 
     def props(self, w, Ns, alpha, phic, f):
+        """density::props with the reference signature (density.h:344): w[0:2M)
+        in, w[2M:6M) out; returns (lnQ, phis)."""
         return self.ctx.props_host(w, Ns, alpha, phic, f)
 
 

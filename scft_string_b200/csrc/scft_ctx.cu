@@ -199,16 +199,22 @@ FieldArgs field_args(scft_ctx *ctx, const int *rep_list)
     return a;
 }
 
+// the kernels' error word: 1, 2 launch geometry (a host bug), 3 a bounded
+// bulk-copy wait gave up (tma.cuh).  It is cleared once reported, so the
+// context stays usable.
 scft_status check_device_err(scft_ctx *ctx)
 {
     int e = 0;
     CK(cudaMemcpyAsync(&e, ctx->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    if (e != 0) {
-        ctx->lasterr = "device kernel reported a launch-geometry error " + std::to_string(e);
-        return SCFT_CUDA_ERROR;
+    if (e == 0) return SCFT_OK;
+    CK(cudaMemsetAsync(ctx->err, 0, sizeof(int), ctx->st));
+    if (e == 3) {
+        ctx->lasterr = "a bounded device wait for a bulk copy gave up";
+        return SCFT_TIMEOUT;
     }
-    return SCFT_OK;
+    ctx->lasterr = "device kernel reported a launch-geometry error " + std::to_string(e);
+    return SCFT_CUDA_ERROR;
 }
 
 // uploads a replica list to the device (pageable copy: staged before return)

@@ -114,3 +114,57 @@ def test_spline_natural_coefficients_by_hand():
     assert np.allclose(c, [0.0, -1.5, 0.0])
     assert np.allclose(b[:2], [1.5, 0.0])
     assert np.allclose(d[:2], [-0.5, 0.5])
+
+
+def _debye(f, x):
+    """Debye function of a block of fraction f: 2 (f x + exp(-f x) - 1) / x^2."""
+    return 2 * (f * x + np.exp(-f * x) - 1) / x**2
+
+
+@pytest.mark.parametrize("f,L,ens", [(0.4, 3.0, 1), (0.5, 2.5, 1), (0.3, 4.0, 2), (0.45, 3.0, 2)])
+def test_weak_single_mode_matches_rpa(f, L, ens):
+    """Linear response of a pure diblock melt (phic = 1, so the homopolymer
+    carries no weight) to W- = eps cos(2 pi x / L), W+ = 0: then wA = W- and
+    wB = -W- (density.h:118-125), and the A density's cos mode is
+    -(S_AA - S_AB) eps with the Debye functions S_AA = g(f), S_AB =
+    (g(1) - g(f) - g(1 - f)) / 2 at x = k^2 / 6 (lengths in R0, diffusion
+    exp(-k^2 ds / 6) per contour step, density.h:79-95).  The pseudo-spectral
+    step is exact for one mode, so the oracle matches to about 1e-9."""
+    m, N, eps = (32, 2, 2), 200, 1e-4
+    D = np.array([L, 1.0, 1.0])
+    M = int(np.prod(m))
+    X = np.arange(m[0]) * L / m[0]
+    w = np.zeros(6 * M)
+    w[:M] = ((eps * np.cos(2 * np.pi * X / L))[:, None, None] * np.ones(m)).ravel()
+    O.Density(m, D, N).props(w, N, 0.1, 1.0, f, ens)
+    phiA = w[2 * M:3 * M].reshape(m)
+    amp = 2 * np.mean(phiA[:, 0, 0] * np.cos(2 * np.pi * X / L))
+    x = (2 * np.pi / L) ** 2 / 6
+    fr = round(N * f) / N
+    pred = -(_debye(fr, x) - 0.5 * (_debye(1, x) - _debye(fr, x) - _debye(1 - fr, x))) * eps
+    assert abs(amp / pred - 1) <= 1e-6, (amp, pred)
+
+
+@pytest.mark.parametrize("ens", [1, 2])
+def test_richardson_step_is_fourth_order(ens):
+    """Global convergence of lnQ in ds: the Richardson combination (4 S_half^2
+    - S_full) / 3 (density.h:129-220) cancels the ds^2 error of the split
+    step, so halving ds divides the error by 16.  Fields strong enough to
+    matter (|W-| up to 5.5); n1 = N/2 and Nh = N/10 stay integers."""
+    m, D = (16, 8, 8), np.array([3.0, 2.0, 2.0])
+    M = int(np.prod(m))
+    X = np.arange(m[0]) * D[0] / m[0]
+    Y = np.arange(m[1]) * D[1] / m[1]
+    wm = (4.0 * np.cos(2 * np.pi * X / D[0]))[:, None, None] + (1.5 * np.sin(2 * np.pi * Y / D[1]))[None, :, None] * np.ones(m)
+    wp = (0.5 * np.cos(4 * np.pi * X / D[0]))[:, None, None] * np.ones(m)
+
+    def lnq(N):
+        w = np.zeros(6 * M)
+        w[:M], w[M:2 * M] = wm.ravel(), wp.ravel()
+        return O.Density(m, D, N).props(w, N, 0.1, 0.8, 0.5, ens)[0]
+
+    ref = lnq(640)
+    err = [abs(lnq(N) - ref) for N in (20, 40, 80, 160)]
+    orders = [np.log2(err[i] / err[i + 1]) for i in range(3)]
+    print("observed orders", orders)
+    assert all(3.8 <= p <= 4.3 for p in orders), orders

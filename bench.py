@@ -133,41 +133,69 @@ def profiled_traffic():
     return None
 
 
+def cpu_props_seconds(m, D, N, wm, wp, alpha, phidb, f, ens, threads, budget_s=10.0, max_calls=20, min_calls=1):
+    """Seconds per FP64 oracle props call (the reference algorithm restated in
+    C, OpenMP over grid points) at the fields wm, wp on `threads` host threads:
+    at least min_calls calls, then more while the time budget lasts and fewer
+    than max_calls were made.  Returns (seconds per call, calls made)."""
+    import numpy as np
+
+    import oracle as O
+    O.set_threads(threads)
+    M = int(np.prod(m))
+    d = O.Density(m, D, N)
+    w = np.zeros(6 * M)
+    w[:M], w[M:2 * M] = np.ravel(wm), np.ravel(wp)
+    fr = round(N * f) / N
+    t0 = time.time()
+    n = 0
+    while n < min_calls or (time.time() - t0 < budget_s and n < max_calls):
+        d.props(w, N, alpha, phidb, fr, ens)
+        n += 1
+    return (time.time() - t0) / n, n
+
+
+def cpu_step_rate(m, D, N, wm, wp, f, threads, budget_s=10.0, min_steps=2, max_steps=50):
+    """Contour steps per second of the FP64 oracle's Richardson step (q and
+    q^dagger advanced by ds, as do_step, density.h:129-220) on `threads` host
+    threads, over a bounded number of steps.  The density sum is not timed, and
+    only the step's scratch is allocated, not the N+1 slices of a props store
+    (6.7 GB at 128^3, N = 200).  Returns (steps per second, steps timed)."""
+    import numpy as np
+
+    import oracle as O
+    O.set_threads(threads)
+    M = int(np.prod(m))
+    d = O.Density(m, D, 2)
+    d.prepare(1.0 / N, np.concatenate([np.ravel(wm), np.ravel(wp)]))
+    n1 = int(round(N * f))
+    q = np.ones(2 * M)
+    t0 = time.time()
+    n = 0
+    while n < min_steps or (time.time() - t0 < budget_s and n < max_steps):
+        q = d.do_step(q, n % N, n1, N - n1)
+        n += 1
+    return n / (time.time() - t0), n
+
+
 def cpu_baseline(cfg, props_per_iter):
     """The FP64 oracle (the reference algorithm restated in C, OpenMP over
     grid points) timed on the host cores: a bounded sample of props calls of
     one replica of the workload."""
-    import numpy as np
-
     import oracle as O
     from scft_string_b200.configs import fields
     cores = os.cpu_count() or 1
-    O.set_threads(cores)
     wm, wp = fields(cfg)
-    M = wm.shape[1]
-    d = O.Density(cfg["m"], cfg["D"], cfg["N"])
-    w = np.zeros(6 * M)
-    w[:M], w[M:2 * M] = wm[1], wp[1]
-    f = round(cfg["N"] * cfg["f"]) / cfg["N"]
-    t0 = time.time()
-    n = 0
-    while n < 3 or (time.time() - t0 < 10 and n < 20):
-        d.props(w, cfg["N"], cfg.get("alpha", 0.1), cfg["phidb"], f, cfg["ens"])
-        n += 1
-    tp = (time.time() - t0) / n
+    args = (cfg["m"], cfg["D"], cfg["N"], wm[1], wp[1], cfg.get("alpha", 0.1), cfg["phidb"], cfg["f"], cfg["ens"])
+    tp, _ = cpu_props_seconds(*args, threads=cores, budget_s=10.0, max_calls=20, min_calls=3)
     # the same on one core (one or two props calls)
-    O.set_threads(1)
-    t1 = time.time()
-    n1 = 0
-    while n1 < 1 or (time.time() - t1 < 8 and n1 < 2):
-        d.props(w, cfg["N"], cfg.get("alpha", 0.1), cfg["phidb"], f, cfg["ens"])
-        n1 += 1
-    tp1 = (time.time() - t1) / n1
+    tp1, _ = cpu_props_seconds(*args, threads=1, budget_s=8.0, max_calls=2)
     O.set_threads(cores)
+    m = cfg["m"]
     return {"value": 1.0 / (props_per_iter * cfg["strn"] * tp), "unit": "string iters/s",
             "value_1core": 1.0 / (props_per_iter * cfg["strn"] * tp1), "props_s_1core": tp1,
             "cores": cores, "kind": "port",
-            "sample": f"{n} props calls of one replica (64^3, N=128, FP64, {cores} threads), "
+            "sample": f"props calls of one replica ({m[0]}x{m[1]}x{m[2]}, N={cfg['N']}, FP64, {cores} threads), "
                       f"{tp:.3f} s each; rate = 1/(props per iteration x replicas x that time) with "
                       f"{props_per_iter:.2f} props per replica per iteration as measured on the GPU",
             "contour_steps_per_s": cfg["N"] / tp}
@@ -221,6 +249,13 @@ def run_uneven(a):
             "roofline": {"bound": "hbm", "achieved": algo / wall / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / wall / 1e9 / peak, "peak_kind": peak_kind,
                          "note": "8 M b algorithmic bytes per contour step, wall time of the whole batch"}}
+    cores = os.cpu_count() or 1
+    c64 = next(c for c in solves if c["m"][0] == 64)
+    wm0, wp0 = noise_fields(c64)
+    rate, n = cpu_step_rate(c64["m"], c64["D"], c64["N"], wm0, wp0, c64["f"], cores, budget_s=10.0)
+    line["cpu_baseline"] = {"contour_steps_per_s": rate, "cores": cores, "kind": "port",
+                            "sample": f"{n} Richardson steps of one 64^3 solve of the batch (N={c64['N']}, FP64, "
+                                      f"{cores} threads); the density sum is not timed"}
     if a.serial_fp64:
         s64 = 0
         w64 = 0.0
@@ -298,6 +333,11 @@ def run_mixed128(a):
     out["fp32_error"] = {"F_per_chain_max": max(dF), "lnQ_rel_max": max(dQ), "rhoA_maxabs": max(drho),
                          "errtot_rel_max": float(np.max(np.abs(e32 - e64) / e64))}
     out["fp32_speedup"] = out["fp32"]["contour_steps_per_s"] / out["fp64"]["contour_steps_per_s"]
+    cores = os.cpu_count() or 1
+    rate, n = cpu_step_rate(c["m"], c["D"], c["N"], wm[0], wp[0], c["f"], cores, budget_s=15.0)
+    out["cpu_baseline"] = {"contour_steps_per_s": rate, "cores": cores, "kind": "port",
+                           "sample": f"{n} Richardson steps of one replica (128^3, FP64, {cores} threads); "
+                                     "the density sum is not timed"}
     print(json.dumps(out))
     return 0
 

@@ -33,3 +33,39 @@ def test_defaults(monkeypatch, argv, steps, warmup):
     assert (a.gpus, a.steps, a.warmup, a.impl, a.precision, a.workload) == (1, steps, warmup, "ours", "fp32",
                                                                             "string")
     assert a.warmup >= 3
+
+
+def test_cpu_props_timing_bounds_the_sample():
+    """The CPU legs time the oracle (test infrastructure) on a bounded sample:
+    at least min_calls calls, at most max_calls."""
+    import numpy as np
+    m, D, N = (8, 8, 8), (2.0, 2.0, 2.0), 20
+    wm = 0.5 * np.cos(2 * np.pi * np.arange(8) / 8)[:, None, None] * np.ones(m)
+    t, n = bench.cpu_props_seconds(m, D, N, wm, np.zeros(m), 0.1, 0.8, 0.5, 1, threads=1, budget_s=0.0,
+                                   max_calls=20, min_calls=3)
+    assert n == 3 and t > 0
+    t, n = bench.cpu_props_seconds(m, D, N, wm, np.zeros(m), 0.1, 0.8, 0.5, 1, threads=1, budget_s=60.0,
+                                   max_calls=4)
+    assert n == 4
+
+
+def test_cpu_step_rate_matches_the_oracle_step():
+    """cpu_step_rate advances q and q^dagger with the oracle's do_step; the
+    step it times is the one props chains (same result as props' slice 1)."""
+    import numpy as np
+
+    import oracle as O
+    m, D, N = (8, 8, 8), (2.0, 2.0, 2.0), 20
+    wm = 0.5 * np.cos(2 * np.pi * np.arange(8) / 8)[:, None, None] * np.ones(m)
+    rate, n = bench.cpu_step_rate(m, D, N, wm, np.zeros(m), 0.5, threads=1, budget_s=0.0, min_steps=2)
+    assert n == 2 and rate > 0
+    M = 512
+    d = O.Density(m, D, N)
+    w = np.zeros(6 * M)
+    w[:M] = wm.ravel()
+    d.props(w, N, 0.1, 0.8, 0.5, 1)
+    s = O.Density(m, D, 2)
+    s.prepare(1.0 / N, w[:2 * M])
+    q1 = s.do_step(np.ones(2 * M), 0, 10, 10)
+    np.testing.assert_allclose(q1[:M], d.q(0, 1), rtol=1e-14)
+    np.testing.assert_allclose(q1[M:], d.q(1, 1), rtol=1e-14)

@@ -22,8 +22,11 @@
 
 #include "scft_b200.h"
 
-/* scft.cu:879 launches this to check that the device answers */
+#ifdef __CUDACC__
+/* scft.cu:879 launches this to check that the device answers (nvcc builds
+ * scft.cu; a host compiler sees only the class) */
 __global__ void print_from_gpu(void) { printf("Testing GPUs: [%d,%d] (From device)\n", threadIdx.x, blockIdx.x); }
+#endif
 
 class density {
     scft_ctx *ctx_ = nullptr;

@@ -5,7 +5,8 @@ include of the shim, and the single-rank mpi.h stand-in that the reference
 build recipe also uses.  The reference sources are read from
 SCFT_REFERENCE_DIR into a temporary directory, never into the repository; the
 test skips where they are absent.  Compile and link only: running the program
-needs a GPU."""
+needs a GPU.  The binding's own host logic (when it makes, reuses and remakes
+a context) is checked against a recording fake of the ABI."""
 import os
 import shutil
 import subprocess

@@ -120,14 +120,17 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per replica contour step from the committed ncu summary."""
+def profiled_traffic(precision="fp32"):
+    """DRAM bytes per replica contour step from the committed ncu summary of
+    the precision's step kernels (None when no capture was summarised)."""
     path = os.path.join(ROOT, "profiles", "step_traffic.txt")
+    key = "dram_bytes_per_replica_step" if precision == "fp32" else f"dram_bytes_per_replica_step_{precision}"
     try:
         with open(path) as fh:
             for line in fh:
-                if line.startswith("dram_bytes_per_replica_step"):
-                    return float(line.split()[1])
+                t = line.split()
+                if len(t) >= 2 and t[0] == key:
+                    return float(t[1])
     except OSError:
         pass
     return None
@@ -181,13 +184,14 @@ def cpu_step_rate(m, D, N, wm, wp, f, threads, budget_s=10.0, min_steps=2, max_s
 def cpu_baseline(cfg, props_per_iter):
     """The FP64 oracle (the reference algorithm restated in C, OpenMP over
     grid points) timed on the host cores: a bounded sample of props calls of
-    one replica of the workload."""
+    one replica of the workload, scaled to string iterations by the props
+    calls per replica and iteration counted in the timed window."""
     import oracle as O
     from scft_string_b200.configs import fields
     cores = os.cpu_count() or 1
     wm, wp = fields(cfg)
     args = (cfg["m"], cfg["D"], cfg["N"], wm[1], wp[1], cfg.get("alpha", 0.1), cfg["phidb"], cfg["f"], cfg["ens"])
-    tp, _ = cpu_props_seconds(*args, threads=cores, budget_s=10.0, max_calls=20, min_calls=3)
+    tp, n = cpu_props_seconds(*args, threads=cores, budget_s=10.0, max_calls=20, min_calls=3)
     # the same on one core (one or two props calls)
     tp1, _ = cpu_props_seconds(*args, threads=1, budget_s=8.0, max_calls=2)
     O.set_threads(cores)
@@ -195,9 +199,10 @@ def cpu_baseline(cfg, props_per_iter):
     return {"value": 1.0 / (props_per_iter * cfg["strn"] * tp), "unit": "string iters/s",
             "value_1core": 1.0 / (props_per_iter * cfg["strn"] * tp1), "props_s_1core": tp1,
             "cores": cores, "kind": "port",
-            "sample": f"props calls of one replica ({m[0]}x{m[1]}x{m[2]}, N={cfg['N']}, FP64, {cores} threads), "
-                      f"{tp:.3f} s each; rate = 1/(props per iteration x replicas x that time) with "
-                      f"{props_per_iter:.2f} props per replica per iteration as measured on the GPU",
+            "sample": f"{n} props calls of one replica ({m[0]}x{m[1]}x{m[2]}, N={cfg['N']}, FP64, {cores} "
+                      f"threads), {tp:.3f} s each; rate = 1/(props per iteration x replicas x that time) "
+                      f"with {props_per_iter:.2f} props per replica per iteration, counted in the timed "
+                      "window; the string coupling (O(replicas x M) per iteration) is not in the sample",
             "contour_steps_per_s": cfg["N"] / tp}
 
 
@@ -446,6 +451,15 @@ def run_adjoint96(a):
 
 
 def run_ours(a, cfg, rank, world, dev):
+    """Iterations k = W..W+K-1 of the string after the W+ prelude and W warm-up
+    iterations, three times over the same window:
+      value  device-resident fields, timed with CUDA events;
+      e2e    the same iterations again from a host copy of the fields at k = W
+             (scft_string_resume), with every replica's fields copied in from
+             pinned host memory and back out in every iteration;
+      cmp    (rank 0 of a 1-GPU run) the same window from the same state at
+             k = W-2 in the other precision batched and in plain FP64 (one
+             replica at a time), two untimed iterations then K timed."""
     import numpy as np
     import torch
 
@@ -465,16 +479,26 @@ def run_ours(a, cfg, rank, world, dev):
         return D.max_over_ranks(v, world, device="cuda")
 
     wm, wp = fields(cfg)
+    strn = cfg["strn"]
     ctx = S.StringSolver(cfg, precision=a.precision, batched=not a.plain, device=dev)
-    for ii in range(cfg["strn"]):
+    for ii in range(strn):
         ctx.set_fields(ii, wm[ii], wp[ii])
     groups, wide, tune_ms = ctx.autotune()     # slot groups and pencil tile width per props round
     ctx.solve_field0_all(5000, 1e-4)           # prelude, scft.cu:1105
     nsterp = 4000                              # scft.cu:1102
+    M = ctx.M
+    W0 = max(2, a.warmup)
+    pinned = lambda: torch.empty((strn, 2 * M), dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    host_w2, host_w = pinned(), pinned()
     ctx.string_begin(nsterp, 1e-3)
-    for _ in range(a.warmup):
+    for k in range(W0):
+        if k == W0 - 2:
+            for ii in range(strn):
+                ctx.get_fields(ii, out=host_w2[ii])
         ctx.string_step()
-    # ---- timed: K iterations with device-resident fields
+    for ii in range(strn):
+        ctx.get_fields(ii, out=host_w[ii])     # the state at k = W
+    # ---- value: K iterations with device-resident fields
     barrier()
     clk = Clocks(dev) if rank == 0 else None
     ctx.reset_stats()
@@ -486,51 +510,57 @@ def run_ours(a, cfg, rank, world, dev):
     clocks = clk.stop() if clk else None
     st = ctx.stats()
     ms_max = max_over_ranks(ms)
-    # ---- e2e: host-owned fields (pinned), H2D + step + D2H every iteration
-    M = ctx.M
-    host = torch.empty((cfg["strn"], 2 * M), dtype=torch.float64, pin_memory=True).numpy()
-    for ii in range(cfg["strn"]):
-        ctx.get_fields(ii, out=host[ii])
+    # ---- e2e: the same iterations from the host copy at k = W; H2D + step + D2H every iteration
+    host = pinned()
+    host[:] = host_w
+    ctx.string_end()
+    ctx.string_resume(W0, nsterp, 1e-3)
     barrier()
     ctx.timer_mark(2)
+    reps_e2e = []
     for _ in range(a.steps):
-        for ii in range(cfg["strn"]):
+        for ii in range(strn):
             ctx.set_fields_2m(ii, host[ii])      # H2D from pinned host memory
-        ctx.string_step()
-        for ii in range(cfg["strn"]):
+        reps_e2e.append(ctx.string_step())
+        for ii in range(strn):
             ctx.get_fields(ii, out=host[ii])     # D2H into pinned host memory
     ctx.timer_mark(3)
     e2e_ms = max_over_ranks(ctx.timer_elapsed_ms(2, 3))
     barrier()
-    out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M,
+    same = all(x["errtot"] == y["errtot"] for x, y in zip(reps, reps_e2e))
+    out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M, W0=W0,
+               e2e_same_iterations=same,
                schedule={"slot_groups": groups, "wide_pencil_tiles": bool(wide),
                          "props_round_ms": dict(zip(["g1_tile1", "g2_tile1", "g1_tile2", "g2_tile2"], tune_ms))})
-    # ---- plain FP64 path on the same state, same first iterations
-    if rank == 0 and world == 1 and not a.no_fp64 and a.precision == "fp32":
-        k2 = min(2, a.steps)
-        ctx64 = S.StringSolver(cfg, precision="fp64", batched=False, device=dev)
-        ctx32 = S.StringSolver(cfg, precision="fp32", batched=True, device=dev)
-        for ii in range(cfg["strn"]):
-            w = host[ii]
-            ctx64.set_fields(ii, w[:M], w[M:])
-            ctx32.set_fields(ii, w[:M], w[M:])
+    # ---- the other precision (batched) and plain FP64 on the same window
+    if rank == 0 and world == 1 and not a.no_fp64:
+        other = "fp64" if a.precision == "fp32" else "fp32"
+        legs = [(f"{other}_batched", other, True)]
+        if not (a.precision == "fp64" and a.plain):
+            legs.append(("fp64_plain", "fp64", False))
         res = {}
-        for name, c in (("fp64_plain", ctx64), ("fp32_batched", ctx32)):
-            c.string_begin(nsterp, 1e-3)
-            c.string_step()  # k = 0 runs FreeE
-            c.string_step()  # k = 1 captures the graphs of the iteration's props rounds
+        for name, prec, batched in legs:
+            c = S.StringSolver(cfg, precision=prec, batched=batched, device=dev)
+            for ii in range(strn):
+                c.set_fields_2m(ii, host_w2[ii])
+            if batched:
+                c.autotune()
+            c.string_resume(W0 - 2, nsterp, 1e-3)
+            c.string_step()
+            c.string_step()  # untimed: graph capture of the iteration's props rounds
             c.reset_stats()
             c.timer_mark(0)
-            for _ in range(k2):
-                c.string_step()
+            rr = [c.string_step() for _ in range(a.steps)]
             c.timer_mark(1)
             t = c.timer_elapsed_ms(0, 1)
             s2 = c.stats()
-            res[name] = dict(iters_per_s=k2 / (t / 1e3),
+            res[name] = dict(iters_per_s=a.steps / (t / 1e3),
                              contour_steps_per_s=s2["contour_steps"] / s2["props_seconds"],
-                             iters=k2)
+                             props_per_replica_iter=s2["props_calls"] / (a.steps * strn),
+                             iters=a.steps, window=f"k={W0}..{W0 + a.steps - 1}",
+                             errtot_last=rr[-1]["errtot"])
             c.close()
-        out["fp64_cmp"] = res
+        out["cmp"] = res
     D.finalize(world)
     return out
 
@@ -552,29 +582,32 @@ def main():
         if rank != 0:
             return 0
         from oracle.refrun import time_iterations
-        # the reference needs ~7 s per iteration of this workload plus a ~3 min
-        # W+ prelude: time at most 5 iterations so the run stays within minutes
-        k_ref = min(a.steps, 5)
-        r = time_iterations(cfg, a.warmup, k_ref)
+        # the same window as our arm: iterations k = W..W+K-1 after the prelude
+        r = time_iterations(cfg, max(2, a.warmup), a.steps)
         if "unavailable" in r:
             print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
             return 0
         v = r["iters_per_s"]
         line = {"metric": METRIC, "value": v, "unit": "string iters/s", "n_gpus": 1,
-                "steps": k_ref, "warmup": a.warmup, "ms_per_step": 1e3 / v,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / v,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded fields, scft_string_b200.configs)",
                 "config": {"workload": cfg["name"], "replicas": cfg["strn"], "grid": list(cfg["m"]),
                            "N": cfg["N"], "ens": cfg["ens"],
+                           "window": f"iterations k={max(2, a.warmup)}..{max(2, a.warmup) + a.steps - 1} "
+                                     "after the W+ prelude",
                            "program": "reference scft.cu built for sm_100a (oracle/build_ref.sh), "
                                       "single rank owning every replica"},
                 "impl": "reference",
-                "cpu_baseline": {"value": v, "unit": "string iters/s", "cores": 1,
-                                 "kind": "reference",
-                                 "sample": "reference program on the GPU (its only implementation "
-                                           "is CUDA); host thread count 1"},
+                "reference_run": {"device": "B200 GPU: the reference's only implementation is CUDA "
+                                            "with cuFFT (it has no CPU path)",
+                                  "host_threads": 1, "timing": "host timestamps printed at the start "
+                                  "of each iteration (KSTART), iterations W..W+K-1",
+                                  "props_calls_seen": r["props_lines"]},
                 "e2e": {"value": v, "unit": "string iters/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        if not a.no_cpu and r.get("props_in_window"):
+            line["cpu_baseline"] = cpu_baseline(cfg, r["props_in_window"] / (a.steps * cfg["strn"]))
         print(json.dumps(line))
         return 0
 
@@ -587,12 +620,14 @@ def main():
     step_bytes = 8 * M * b                              # algorithmic bytes per replica contour step
     achieved = step_bytes * st["contour_steps"] / st["props_seconds"] / 1e9
     peak, peak_kind = peaks()
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(a.precision)
     from scft_string_b200 import dist as D
     value = D.job_rate(a.steps, world, r["ms"])
     props_per_iter = st["props_calls"] / (a.steps * cfg["strn"])
     import math
     flops = 30.0 * M * math.log2(M) * st["contour_steps"] / st["props_seconds"] / 1e12
+    W0 = r["W0"]
+    window = f"iterations k={W0}..{W0 + a.steps - 1} after the W+ prelude"
     line = {
         "metric": METRIC, "value": value, "unit": "string iters/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["ms"] / a.steps,
@@ -602,8 +637,7 @@ def main():
         "config": {"workload": cfg["name"], "replicas": cfg["strn"], "grid": list(cfg["m"]),
                    "N": cfg["N"], "ens": cfg["ens"], "precision": a.precision,
                    "batched": not a.plain, "parallelism": f"replicas-only x{world}",
-                   "schedule": r["schedule"],
-                   "window": f"iterations k={a.warmup}..{a.warmup + a.steps - 1} after the W+ prelude",
+                   "schedule": r["schedule"], "window": window,
                    "l2": "inputs larger than L2 (propagator store "
                          f"{cfg['strn'] * (cfg['N'] + 1) * 2 * M * b / 1e9:.1f} GB per props round)"},
         "errtot_last": reps[-1]["errtot"], "props_per_replica_iter": props_per_iter,
@@ -611,22 +645,27 @@ def main():
         "gpu_launches": st["kernel_launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": None if traffic is None else traffic * 1.0,
+                     "traffic": traffic,
                      "unit_of_work": "replica contour step (q and q^dagger advanced by ds)",
                      "algorithmic_bytes_per_unit": step_bytes,
-                     "fp32_tflops": flops},
+                     "fp32_tflops" if b == 4 else "fp64_tflops": flops},
         "e2e": {"value": world * a.steps / (r["e2e_ms"] / 1e3), "unit": "string iters/s",
                 "h2d_bytes_per_step": cfg["strn"] * 2 * M * 8,
                 "d2h_bytes_per_step": cfg["strn"] * 2 * M * 8,
-                "window": f"iterations k={a.warmup + a.steps}..{a.warmup + 2 * a.steps - 1}, right after the "
-                          "device-resident window; later iterations need fewer inner W+ iterations, so "
-                          "this rate can exceed value"},
+                "window": window + " (the same iterations as value, continued from a host copy of the "
+                          "fields at their start)",
+                "same_iterations_as_value": r["e2e_same_iterations"]},
         "clocks": r["clocks"],
     }
-    if "fp64_cmp" in r:
-        c = r["fp64_cmp"]
-        line["fp64_plain_cmp"] = c
-        line["speedup_vs_fp64_plain"] = c["fp32_batched"]["iters_per_s"] / c["fp64_plain"]["iters_per_s"]
+    if "cmp" in r:
+        c = r["cmp"]
+        line["same_window_cmp"] = c
+        if a.precision == "fp32" and "fp64_plain" in c:
+            line["speedup_vs_fp64_plain"] = value / c["fp64_plain"]["iters_per_s"]
+        if "fp64_plain" in c and "fp32_batched" in c:
+            line["fp32_batched_vs_fp64_plain"] = c["fp32_batched"]["iters_per_s"] / c["fp64_plain"]["iters_per_s"]
+        if a.precision == "fp64" and not a.plain and "fp64_plain" in c:
+            line["fp64_batched_vs_fp64_plain"] = value / c["fp64_plain"]["iters_per_s"]
     if world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(cfg, props_per_iter)
     print(json.dumps(line))

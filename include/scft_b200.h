@@ -102,6 +102,11 @@ const char *scft_status_string(scft_status s);
  * (scft.cu:1062). */
 scft_status scft_set_fields(scft_ctx *ctx, int ii, const double *w2M);
 scft_status scft_get_fields(const scft_ctx *ctx, int ii, double *w2M);
+/* Fields and boxes of every replica of src into ctx (no reference
+ * counterpart): device to device, for contexts of the same grid and replica
+ * count, e.g. an FP32 context handing its string to an FP64 one for the last
+ * iterations of a solve.  Waits for src's stream. */
+scft_status scft_copy_fields(scft_ctx *ctx, const scft_ctx *src);
 /* Concentrations of the last props of replica ii: [phiA, phiB, phih, phicB]
  * (4*M doubles, W[ii]+2M of the reference), lnQ and phis[5]. */
 scft_status scft_get_conc(const scft_ctx *ctx, int ii, double *out4M, double *lnQ, double *phis);
@@ -140,6 +145,13 @@ scft_status scft_string_begin(scft_ctx *ctx, int doii, int maxIter, double errTo
 scft_status scft_string_step(scft_ctx *ctx, scft_iter_report *rep, double *errs, double *errs3,
                              int *done);
 scft_status scft_string_end(scft_ctx *ctx, int *k_out);
+/* scft_string_begin with the iteration counter set to k0 (no reference
+ * counterpart): continues a string run from fields saved at iteration k0
+ * (scft_save_checkpoint, or host copies), so that the FreeE cadence
+ * (k % 50 == 0, scft.cu:761, 778) and the spring steps (k < springsteps,
+ * scft.cu:594) follow the uninterrupted run.  The mixing parameter restarts
+ * at 0.05, the value the reference's loop keeps (scft.cu:563, 793-797). */
+scft_status scft_string_resume(scft_ctx *ctx, int doii, int maxIter, double errTol, int k0);
 /* FreeE (scft.cu:812-853): W+ re-solve (100 iterations, 1e-4) and props of
  * every replica, then F = -lnQ + <chi phiA phiB - wA phiA - wB phiB>.
  * Arrays have strn entries; any may be NULL. */
@@ -219,19 +231,27 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
 
 /* ---- allocation-free step (no counterpart in the reference) ------------ */
 /* One Richardson contour step for callers that cannot allocate device memory
- * when they need it (a host recording work for later replay, a real-time loop
- * that must not stall on the allocator, a framework that owns every device
- * allocation).  Same kernels and result as scft_do_step, but every working
- * buffer lives in one static __device__ array of 4.2 MB, so it calls no
- * cudaMalloc/cudaFree.  All pointers are the caller's device memory: w2M =
- * [W-, W+], in2M = [q(s), q^dagger(s)], out2M = [q(s+1), q^dagger(s+1)], each
- * 2*M doubles; f is the A fraction as in scft_problem; stream may be NULL.
- * Limits: FP64, M <= 32768, each m_i <= 64 (BAD_INPUT beyond).  The first
- * call on a device looks up the array's address (cudaGetSymbolAddress): make
- * it before any stream capture.  Calls share the array, so calls that overlap
- * on the GPU race; the call waits for its stream before returning. */
+ * when they need a step: a real-time loop that must not stall on the
+ * allocator (cudaMalloc can synchronise the device), or a framework that owns
+ * every device allocation through its own pool.  Same kernels and result as
+ * scft_do_step, but every working buffer lives in one static __device__
+ * array of 4.2 MB, so it calls no cudaMalloc/cudaFree.  All pointers are the
+ * caller's device memory: w2M = [W-, W+], in2M = [q(s), q^dagger(s)], out2M =
+ * [q(s+1), q^dagger(s+1)], each 2*M doubles; f is the A fraction (0..1) as in
+ * scft_problem; stream may be NULL.  Limits: FP64, M <= 32768, each m_i <= 64
+ * (BAD_INPUT beyond).  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress): make it before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race; the call waits for
+ * its stream before returning. */
 scft_status scft_do_step_noalloc(const int *m, const double *D, int N, double f, const double *w2M,
                                  const double *in2M, double *out2M, int s, void *stream);
+
+/* ---- failure-path self-test (no reference counterpart) ----------------- */
+/* Runs one bounded device wait on a barrier that no copy completes, so the
+ * wait gives up after `polls` polls exactly as a wait on a lost bulk copy
+ * would (the step kernels allow 2^20 polls).  Returns SCFT_TIMEOUT and clears
+ * the error word, leaving the context usable; for tests of the error path. */
+scft_status scft_selftest_timeout(scft_ctx *ctx, int polls);
 
 /* ---- statistics (no reference counterpart) ---------------------------- */
 /* Records CUDA event `slot` (0..3) on the context's stream; elapsed device

@@ -41,6 +41,8 @@ def time_iterations(cfg: dict, warmup: int, steps: int, timeout: float = 1500.0,
     wm, wp = fields(cfg)
     stamps = {}
     props_lines = 0
+    props_in_window = 0
+    kcur = -1
     t0 = time.time()
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "input.dat"), "w") as fh:
@@ -55,9 +57,12 @@ def time_iterations(cfg: dict, warmup: int, steps: int, timeout: float = 1500.0,
             for line in proc.stdout:
                 if line.startswith("PROPS"):
                     props_lines += 1
+                    if warmup <= kcur < warmup + steps:
+                        props_in_window += 1
                 elif line.startswith("KSTART"):
                     _, k, t = line.split()
                     stamps[int(k)] = float(t)
+                    kcur = int(k)
                     if int(k) >= warmup + steps and not stopped:
                         proc.send_signal(signal.SIGINT)
                         stopped = True
@@ -74,4 +79,4 @@ def time_iterations(cfg: dict, warmup: int, steps: int, timeout: float = 1500.0,
                                 f"(rc={proc.returncode})")
     sec = stamps[warmup + steps] - stamps[warmup]
     return dict(seconds=sec, iters=steps, iters_per_s=steps / sec, props_lines=props_lines,
-                wall=time.time() - t0)
+                props_in_window=props_in_window, wall=time.time() - t0)

@@ -80,7 +80,8 @@ EXPORTS = [
     "scft_stress", "scft_dF_dchi", "scft_relax_cell", "scft_do_step_noalloc",
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
     "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
-    "scft_gradients", "scft_props_ckpt", "scft_checkpoint_info",
+    "scft_gradients", "scft_props_ckpt", "scft_checkpoint_info", "scft_string_resume",
+    "scft_selftest_timeout", "scft_copy_fields",
 ]
 
 _lib = None
@@ -118,6 +119,9 @@ def lib():
     L.scft_string_begin.argtypes = [vp, C.c_int, C.c_int, C.c_double]
     L.scft_string_step.argtypes = [vp, C.POINTER(IterReport), _dp, _dp, _ip]
     L.scft_string_end.argtypes = [vp, _ip]
+    L.scft_string_resume.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int]
+    L.scft_selftest_timeout.argtypes = [vp, C.c_int]
+    L.scft_copy_fields.argtypes = [vp, vp]
     L.scft_free_energy.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
     L.scft_last_free_energy.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
     L.scft_spline_derivs.argtypes = [vp, _dp, C.POINTER(_dp), C.c_int, C.c_int, _ip,
@@ -223,6 +227,11 @@ class Context:
         """Replica ii's [W-, W+] from one contiguous 2M array (no staging copy)."""
         self._ck(lib().scft_set_fields(self.h, int(ii), _p(w2m)))
 
+    def copy_fields_from(self, other):
+        """Fields and boxes of every replica of context `other` (same grid and
+        replica count), device to device."""
+        self._ck(lib().scft_copy_fields(self.h, other.h))
+
     def get_conc(self, ii):
         """(concentrations [phiA, phiB, phih, phicB] as 4M doubles, lnQ, phis[5]) of
         replica ii's last props: W[ii][2M:6M), lnQ and phis of density::props
@@ -306,6 +315,11 @@ class Context:
     def string_begin(self, maxIter, errTol=1e-3, doii=-1):
         """Starts solve_field one iteration at a time (see string_step)."""
         self._ck(lib().scft_string_begin(self.h, int(doii), int(maxIter), float(errTol)))
+
+    def string_resume(self, k0, maxIter, errTol=1e-3, doii=-1):
+        """string_begin with the iteration counter at k0: continues a run from
+        fields saved at iteration k0 with the same FreeE cadence."""
+        self._ck(lib().scft_string_resume(self.h, int(doii), int(maxIter), float(errTol), int(k0)))
 
     def string_step(self):
         """One iteration of the solve_field loop (scft.cu:592-806): its record,
@@ -465,6 +479,11 @@ class Context:
         """Boxes and fields of every replica from a binary checkpoint (hash,
         grid and replica count checked)."""
         self._ck(lib().scft_load_checkpoint(self.h, os.fsencode(path)))
+
+    def selftest_timeout(self, polls=1000):
+        """Status code of one bounded device wait that nothing completes
+        (SCFT_TIMEOUT = 4 expected); the context stays usable."""
+        return int(lib().scft_selftest_timeout(self.h, int(polls)))
 
     def timer_mark(self, slot):
         """Records CUDA event `slot` on the context's stream."""

@@ -13,8 +13,8 @@ EXE = os.path.join(HERE, "scft_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu", "noalloc.cu",
-              "density_ckpt.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh"]
+              "density_ckpt.cu", "reg64.cu"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh", "reg64.cuh"]
 
 
 def _stale(target, deps):

@@ -60,7 +60,15 @@ struct PropsLaunch {
     int ptile_wide;  // tensor-map x pass with tiles of twice the default width
     int pencil_tma_smem_wide;
     const CUtensorMap *tmap_wide;  // the same spectra with the wide tile box
+    int reg;         // 64^3 FP32: register-resident step kernels (reg64.cu) instead of the shared-memory ones
 };
+
+// register-resident 64^3 FP32 step kernels (reg64.cu)
+bool reg64_applicable(int m0, int m1, int m2);
+int reg64_set_smem();
+void reg64_combine(const PropsArgs<float> &a, int nslots, int s, int mode, cudaStream_t st);
+void reg64_mid(const PropsArgs<float> &a, int nslots, int s, cudaStream_t st);
+void reg64_pencil(const PropsArgs<float> &a, int nslots, int both, cudaStream_t st);
 
 void pf_smem_bytes(int id, int fp32, int &mid, int &comb);
 
@@ -82,6 +90,8 @@ template <typename T>
 int launch_prepare(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st);
 template <typename T>
 int launch_qsums(const PropsArgs<T> &a, const PropsLaunch &L, cudaStream_t st);
+// one bounded wait on a barrier that nothing completes: error 3 after `polls` polls
+int launch_wait_selftest(int *err, unsigned polls, cudaStream_t st);
 
 // ------------------------------------------------------------------ stress (adjoint)
 constexpr int kStressPairs = 16;

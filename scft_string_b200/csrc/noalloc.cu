@@ -1,27 +1,29 @@
 // noalloc.cu -- one Richardson contour step that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc at the moment they need a propagator
-// step: a host that is recording work into a stream for later replay, a
-// real-time loop that must not stall on the allocator (cudaMalloc can
-// synchronise the device), or an embedding framework that owns every device
-// allocation through its own pool and forbids foreign ones.  For them,
-// scft_do_step_noalloc runs the same kernels as scft_do_step (the
-// runtime-shaped k_prepare, k_combine, k_pencil and k_mid) with all of
-// their working buffers -- spectra, E tables, the full-step partial, the two
-// propagator slices, FFT twiddles, diffusion factors and the error word -- in
-// one file-scope __device__ array of kNoAllocBytes.  The caller passes only
-// its own device buffers for the fields, the input slice and the output slice.
+// step: a real-time loop that must not stall on the allocator (cudaMalloc
+// can synchronise the whole device), or an embedding framework that owns
+// every device allocation through its own pool and forbids foreign ones.
+// For them, scft_do_step_noalloc runs the same runtime-shaped kernels as
+// scft_do_step (k_prepare, k_combine, k_pencil, k_mid) with all of their
+// working buffers -- spectra, E tables, the full-step partial, the two
+// propagator slices, FFT twiddles, diffusion factors and the error word --
+// in one file-scope __device__ array of kNoAllocBytes.  The caller passes
+// only its own device buffers for the fields, the input slice and the
+// output slice.
 //
 // Limits and sharing: FP64, M = m0*m1*m2 <= 32768 and every m_i <= 64 with
 // prime factors <= 7.  The array lives on every GPU that loads this library
 // until the process exits.  All calls share it and it keeps the last call's
 // contents, so calls that overlap on the GPU (different streams or threads
-// without ordering) race; serialise them.
+// without ordering) race; serialise them.  The call waits for its stream
+// before it returns (it reads the kernels' error word).
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/scft_b200.h"
 #include "kernels.h"
@@ -39,8 +41,12 @@ constexpr size_t kNoAllocBytes = kNoAllocDoubles * sizeof(double);
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 static_assert(sizeof(g_noalloc_scratch) == kNoAllocBytes, "scratch size");
 
-// device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
+// device address of g_noalloc_scratch per device, from cudaGetSymbolAddress;
+// each entry is filled once, under its own once-flag, by the first call on
+// that device (host threads racing on a first call wait for the winner)
 void *g_scratch_addr[kNoAllocMaxDevices];
+cudaError_t g_scratch_rc[kNoAllocMaxDevices];
+std::once_flag g_scratch_once[kNoAllocMaxDevices];
 
 bool factor7(int n, Plan1D &p)
 {
@@ -105,6 +111,7 @@ extern "C" scft_status scft_do_step_noalloc(const int *m, const double *D, int N
                                             const double *in2M, double *out2M, int s, void *stream)
 {
     if (!m || !D || !w2M || !in2M || !out2M || N < 1 || s < 0 || s >= N) return SCFT_BAD_INPUT;
+    if (!(f >= 0.0 && f <= 1.0)) return SCFT_BAD_INPUT;  // as scft_create
     for (int i = 0; i < 3; i++)
         if (m[i] < 1 || m[i] > kNoAllocMaxAxis || !(D[i] > 0)) return SCFT_BAD_INPUT;
     const long Ml = (long)m[0] * m[1] * m[2];
@@ -144,11 +151,12 @@ extern "C" scft_status scft_do_step_noalloc(const int *m, const double *D, int N
     // set-up on first use on this device: the array's device address
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return SCFT_CUDA_ERROR;
-    if (!g_scratch_addr[dev]) {
+    std::call_once(g_scratch_once[dev], [dev] {
         void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SCFT_CUDA_ERROR;
+        g_scratch_rc[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         g_scratch_addr[dev] = p;
-    }
+    });
+    if (g_scratch_rc[dev] != cudaSuccess || !g_scratch_addr[dev]) return SCFT_CUDA_ERROR;
     double *base = static_cast<double *>(g_scratch_addr[dev]);
     const size_t M = g.M;
     int *err = reinterpret_cast<int *>(base);     // first 64 doubles: error word and slot map
@@ -172,8 +180,7 @@ extern "C" scft_status scft_do_step_noalloc(const int *m, const double *D, int N
     a.slot_rep = slot_rep;  // slot 0 -> replica 0, the caller's fields
     a.W = w2M;
     a.etab = etab;
-    // slice s of the kernels' propagator store is the first slice of `hist`
-    a.hist = reinterpret_cast<double *>(reinterpret_cast<uintptr_t>(hist) - (uintptr_t)s * 2 * M * sizeof(double));
+    a.hist = hist;
     a.spec = reinterpret_cast<cplx<double> *>(spec);
     a.pbuf = pbuf;
     a.tw = tw;
@@ -181,7 +188,16 @@ extern "C" scft_status scft_do_step_noalloc(const int *m, const double *D, int N
     a.invM = 1.0 / g.M;
     a.Mreal = (double)g.M;
     a.err = err;
-    launch_single_step<double>(a, L, s, st);
+    // E tables of the whole chain (ds = 1/N), then a one-step chain segment
+    // whose store holds only slices s and s+1: its geometry counts contour
+    // steps from s, so n1 and n2 shrink by s and each step still picks the E
+    // table of its absolute index
+    launch_prepare<double>(a, L, st);
+    PropsArgs<double> seg = a;
+    seg.g.Ns = 1;
+    seg.g.n1 = g.n1 - s;
+    seg.g.n2 = g.n2 - s;
+    launch_chain<double>(seg, L, 2, st);
     if (cudaGetLastError() != cudaSuccess) return SCFT_CUDA_ERROR;
     if (cudaMemcpyAsync(out2M, hist + 2 * M, sizeof(double) * 2 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return SCFT_CUDA_ERROR;

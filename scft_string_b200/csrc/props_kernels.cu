@@ -603,6 +603,31 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     if (threadIdx.x == 0) tma_store_wait_read();
 }
 
+// ---------------------------------------------------------------- bounded-wait self-test
+// One CTA waits on an mbarrier that expects 16 transaction bytes no copy will
+// deliver (none is issued), so every thread's wait runs out after `polls`
+// polls, records error 3 in the error word and returns: the path a lost bulk
+// copy takes, exercised without any copy in flight.
+__global__ void k_wait_selftest(int *err, uint32_t polls)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+        mbar_expect_tx(&bar, 16);
+    }
+    __syncthreads();
+    mbar_wait(&bar, 0, err, polls);
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_inval(&bar);
+}
+
+int launch_wait_selftest(int *err, unsigned polls, cudaStream_t st)
+{
+    k_wait_selftest<<<1, 32, 0, st>>>(err, polls);
+    return 1;
+}
+
 // ---------------------------------------------------------------- Q and densities
 __device__ __forceinline__ double block_sum(double v, double *sh)
 {
@@ -797,9 +822,19 @@ __global__ void k_dfinal(PropsArgs<T> a, int nblk)
 // MT bounds the CTA size of the FFT kernels.  Shapes with compile-time
 // instantiations (cubic 32..128 and 64x64x96) use MT threads exactly; the
 // runtime-shaped kernels use 256 (or 1024 for slabs too large for 256).
+// the 64^3 FP32 shape with L.reg set runs the register-resident kernels of reg64.cu
+template <typename T, int F0, int F1, int F2>
+constexpr bool kReg64 = sizeof(T) == 4 && F0 == 64 && F1 == 64 && F2 == 64;
+
 template <typename T, int MT, int F0, int F1, int F2>
 void launch_combine(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s, int mode, cudaStream_t st)
 {
+    if constexpr (kReg64<T, F0, F1, F2>) {
+        if (L.reg) {
+            reg64_combine(a, gs.z, s, mode, st);
+            return;
+        }
+    }
     if constexpr (F1 != 0) {
         if (L.pf) {
             k_combine_pf<T, MT, F0, F1, F2><<<gs, MT, L.combine_pf_smem, st>>>(a, s, mode);
@@ -812,6 +847,12 @@ void launch_combine(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s,
 template <typename T, int MT, int F0, int F1, int F2>
 void launch_mid(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s, cudaStream_t st)
 {
+    if constexpr (kReg64<T, F0, F1, F2>) {
+        if (L.reg) {
+            reg64_mid(a, gs.z, s, st);
+            return;
+        }
+    }
     if constexpr (F1 != 0) {
         if (L.pf) {
             k_mid_pf<T, MT, F0, F1, F2><<<gs, MT, L.mid_pf_smem, st>>>(a, s);
@@ -824,6 +865,12 @@ void launch_mid(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gs, int s, cud
 template <typename T, int MT, int F0, int F1, int F2>
 void launch_pencil(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gp, int both, cudaStream_t st)
 {
+    if constexpr (kReg64<T, F0, F1, F2>) {
+        if (L.reg) {
+            reg64_pencil(a, gp.z, both, st);
+            return;
+        }
+    }
     if constexpr (F1 != 0) {
         if (L.tma_pencil) {
             // tile width: kTile columns, or twice that (two butterflies per
@@ -915,7 +962,12 @@ int set_smem_mt(const PropsLaunch &L)
             e5 = cudaFuncSetAttribute(k_mid_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.mid_pf_smem);
         }
     }
-    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess && e5 == cudaSuccess) ? 0 : -1;
+    int e6 = 0;
+    if constexpr (kReg64<T, F0, F1, F2>) e6 = reg64_set_smem();
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess && e5 == cudaSuccess &&
+            e6 == 0)
+               ? 0
+               : -1;
 }
 
 // shared-memory bytes of the prefetching slab kernels for a fixed shape

@@ -659,6 +659,9 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
     const int rt_slab_threads = L.slab_threads, rt_pencil_threads = L.pencil_threads;
     L.fixed = fixed_shape_id(g.m0, g.m1, g.m2);
     if (L.fixed) L.slab_threads = L.pencil_threads = fixed_shape_threads(L.fixed);
+    // 64^3 FP32: register-resident step kernels (reg64.cu) unless SCFT_NO_REG=1
+    L.reg = (T == 4 && reg64_applicable(g.m0, g.m1, g.m2)) ? 1 : 0;
+    if (const char *ev = getenv("SCFT_NO_REG")) L.reg = ev[0] == '1' ? 0 : L.reg;
     L.pf = 0;
     if (L.fixed) {
         pf_smem_bytes(L.fixed, T == 4, L.mid_pf_smem, L.combine_pf_smem);
@@ -838,6 +841,29 @@ scft_status scft_get_fields(const scft_ctx *cctx, int ii, double *w2M)
     return SCFT_OK;
 }
 
+scft_status upload_box(scft_ctx *ctx, int r, const double *D);
+
+scft_status scft_copy_fields(scft_ctx *ctx, const scft_ctx *src)
+{
+    if (!ctx || !src || ctx == src) return SCFT_BAD_INPUT;
+    const Geo &a = ctx->g, &b = src->g;
+    if (ctx->strn != src->strn || a.m0 != b.m0 || a.m1 != b.m1 || a.m2 != b.m2) {
+        ctx->lasterr = "scft_copy_fields: the contexts differ in grid or replica count";
+        return SCFT_BAD_INPUT;
+    }
+    CK(cudaStreamSynchronize(src->st));  // the source's pending updates of its fields
+    CK(cudaMemcpyAsync(ctx->W, src->W, sizeof(double) * 2 * ctx->M * ctx->strn, cudaMemcpyDefault, ctx->st));
+    for (int r = 0; r < ctx->strn; r++) {
+        const double *D = &src->Dr[3 * (size_t)r];
+        if (D[0] != ctx->Dr[3 * (size_t)r] || D[1] != ctx->Dr[3 * (size_t)r + 1] || D[2] != ctx->Dr[3 * (size_t)r + 2]) {
+            scft_status s = upload_box(ctx, r, D);
+            if (s != SCFT_OK) return s;
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCFT_OK;
+}
+
 scft_status scft_get_conc(const scft_ctx *cctx, int ii, double *out4M, double *lnQ, double *phis)
 {
     scft_ctx *ctx = const_cast<scft_ctx *>(cctx);
@@ -1000,6 +1026,24 @@ scft_status scft_string_begin(scft_ctx *ctx, int doii, int maxIter, double errTo
     if (ctx->p.fix[1] == 1) ctx->doiis[ctx->strn - 1] = 0;
     std::fill(S.steps.begin(), S.steps.end(), 0);
     return SCFT_OK;
+}
+
+scft_status scft_string_resume(scft_ctx *ctx, int doii, int maxIter, double errTol, int k0)
+{
+    if (!ctx || k0 < 0) return SCFT_BAD_INPUT;
+    scft_status s = scft_string_begin(ctx, doii, maxIter, errTol);
+    if (s != SCFT_OK) return s;
+    ctx->sf.k = k0;
+    return SCFT_OK;
+}
+
+scft_status scft_selftest_timeout(scft_ctx *ctx, int polls)
+{
+    if (!ctx || polls < 1) return SCFT_BAD_INPUT;
+    launch_wait_selftest(ctx->err, (unsigned)polls, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    CK(cudaGetLastError());
+    return check_device_err(ctx);
 }
 
 // one k-pass of the solve_field loop, scft.cu:592-806
@@ -2170,7 +2214,7 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
     };
     double best = 0;
     int best_g = 1, best_w = 0;
-    const int nw = ctx->L.tmap_wide ? 2 : 1;
+    const int nw = (ctx->L.tmap_wide && !ctx->L.reg) ? 2 : 1;  // the register kernels have no pencil tiles
     for (int c = 0; c < 4; c++) {
         const int ng = 1 + (c & 1), wide = c >> 1;
         if (times_ms) times_ms[c] = -1;

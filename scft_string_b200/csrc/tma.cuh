@@ -55,12 +55,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
     return ok != 0;
 }
 
-// every thread waits for phase `phase` of `bar`; bounded
-__device__ __forceinline__ void mbar_wait(uint64_t *bar, uint32_t phase, int *err)
+// every thread waits for phase `phase` of `bar`; bounded by `limit` polls
+__device__ __forceinline__ void mbar_wait(uint64_t *bar, uint32_t phase, int *err, uint32_t limit = kSpinLimit)
 {
-    for (uint32_t i = 0; i < kSpinLimit; i++)
+    for (uint32_t i = 0; i < limit; i++)
         if (mbar_try_wait(bar, phase)) return;
     *err = 3;
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 }  // namespace scft

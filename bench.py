@@ -38,8 +38,16 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="one replica at a time")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="string", choices=["string", "uneven24", "mixed128", "adjoint96"],
-                    help="uneven24: the 24 independent solves of mixed grids and N, run concurrently")
+    ap.add_argument("--workload", default="string",
+                    choices=["string", "uneven24", "mixed128", "adjoint96", "tolerance"],
+                    help="uneven24: the 24 independent solves of mixed grids and N, run concurrently; "
+                         "tolerance: the string run to RMS error --tol (time to the metric's error clause)")
+    ap.add_argument("--switch", type=float, default=3e-5,
+                    help="tolerance: errtot at which the FP32 iterations hand the string to FP64")
+    ap.add_argument("--max-iters", type=int, default=4000,
+                    help="tolerance: string iteration cap (the reference's nsterp, scft.cu:1102)")
+    ap.add_argument("--time-limit", type=float, default=0.0,
+                    help="tolerance: stop (reached = false) after this many wall seconds (0: none)")
     ap.add_argument("--tol", type=float, default=1e-5, help="uneven24: RMS residual target")
     ap.add_argument("--start", default="lamellar", choices=["lamellar", "hex"],
                     help="adjoint96: start field of the saddle point search")
@@ -277,6 +285,111 @@ def run_uneven(a):
         line["serial_fp64"] = {"wall_s": w64, "contour_steps_per_s": s64 / w64}
         line["speedup_vs_serial_fp64_wall"] = w64 / wall
     print(json.dumps(line))
+    return 0
+
+
+def run_tolerance(a):
+    """Time to the metric's error clause on the 16-replica 64^3 string: the
+    reference's solve_field iterations (scft.cu:592-806; its loop never stops
+    on the error, scft.cu:563) run until errtot = sqrt(mean errs3^2)
+    (scft.cu:764-765) <= --tol, or --max-iters.
+      --precision fp32: FP32 batched iterations until errtot <= --switch (or
+        no 1 % progress over 200 iterations), then the fields go device to
+        device to an FP64 batched context that continues the same run (same k)
+        to --tol; F per replica from a final FP64 FreeE;
+      --precision fp64: FP64 batched from the start.
+    Device time per phase (CUDA events on each context's stream), the errtot
+    history, F per replica, and -- at the hand-over -- the FP32 errors
+    against FP64 at identical fields."""
+    import numpy as np
+    import torch
+
+    import scft_string_b200 as S
+    from scft_string_b200.configs import STRING_64, fields
+    torch.cuda.set_device(0)
+    cfg = dict(STRING_64)
+    strn, M = cfg["strn"], int(np.prod(cfg["m"]))
+    wm, wp = fields(cfg)
+    t_wall = time.time()
+    first = S.StringSolver(cfg, precision=a.precision, batched=True)
+    for ii in range(strn):
+        first.set_fields(ii, wm[ii], wp[ii])
+    first.autotune()
+    first.timer_mark(0)
+    first.solve_field0_all(5000, 1e-4)  # prelude, scft.cu:1105
+    first.timer_mark(1)
+    prelude_ms = first.timer_elapsed_ms(0, 1)
+    hist = []
+
+    def phase(ctx, k0, stop_tol, stall):
+        ctx.string_resume(k0, a.max_iters, 1e-3)
+        ctx.reset_stats()
+        ctx.timer_mark(2)
+        best, best_k, k = float("inf"), k0, k0
+        while k < a.max_iters:
+            r = ctx.string_step()
+            hist.append((r["k"], r["errtot"]))
+            k = r["k"] + 1
+            if r["errtot"] < 0.99 * best:
+                best, best_k = r["errtot"], k
+            if r["errtot"] <= stop_tol or (stall and k - best_k >= 200):
+                break
+            if a.time_limit > 0 and time.time() - t_wall > a.time_limit:
+                out["time_limited"] = True
+                break
+        ctx.timer_mark(3)
+        st = ctx.stats()
+        return k, dict(iters=k - k0, seconds=ctx.timer_elapsed_ms(2, 3) / 1e3, errtot_end=hist[-1][1],
+                       props_per_replica_iter=st["props_calls"] / max(1, (k - k0) * strn),
+                       contour_steps_per_s=st["contour_steps"] / max(1e-30, st["props_seconds"]))
+
+    out = {"workload": "tolerance: " + cfg["name"], "tol": a.tol, "mode": a.precision, "max_iters": a.max_iters,
+           "prelude_s": prelude_ms / 1e3}
+    if a.precision == "fp32":
+        k, p32 = phase(first, 0, a.switch, True)
+        out["phase_fp32"] = p32
+        W = [np.ascontiguousarray(first.get_fields(ii)) for ii in range(strn)]
+        # FP32 errors against FP64 at the hand-over fields
+        one64 = S.StringSolver(dict(cfg, strn=1), precision="fp64")
+        one32 = S.StringSolver(dict(cfg, strn=1), precision="fp32")
+        dF, dq, dr, dd = [], [], [], []
+        for w in W:
+            F64, q64, r64 = f_per_chain(one64, cfg, w)
+            c64, _, _ = one64.get_conc(0)
+            F32, q32, r32 = f_per_chain(one32, cfg, w)
+            c32, _, _ = one32.get_conc(0)
+            d64 = cfg["chi"] * (c64[M:2 * M] - c64[:M]) - 2 * w[:M]
+            d32 = cfg["chi"] * (c32[M:2 * M] - c32[:M]) - 2 * w[:M]
+            dF.append(abs(F32 - F64))
+            dq.append(abs(q32 - q64) / max(1e-300, abs(q64)))
+            dr.append(float(np.abs(r32 - r64).max()))
+            dd.append(float(np.sqrt(np.mean((d32 - d64) ** 2))))
+        one64.close()
+        one32.close()
+        out["fp32_errors_at_handover"] = {"F_per_chain": dF, "lnQ_rel": dq, "rhoA_maxabs": dr,
+                                          "exchange_residual_rms_diff": dd}
+        second = S.StringSolver(cfg, precision="fp64", batched=True)
+        second.autotune()
+        second.copy_fields_from(first)
+        first.close()
+        if not out.get("time_limited"):
+            k, p64 = phase(second, k, a.tol, False)
+            out["phase_fp64"] = p64
+        last = second
+    else:
+        k, p64 = phase(first, 0, a.tol, False)
+        out["phase_fp64"] = p64
+        last = first
+    fe = last.free_energy()
+    out["reached"] = bool(hist and hist[-1][1] <= a.tol)
+    out["iterations"] = k
+    out["time_to_tol_s"] = sum(out[p]["seconds"] for p in ("phase_fp32", "phase_fp64") if p in out)
+    out["time_to_tol_with_prelude_s"] = out["time_to_tol_s"] + out["prelude_s"]
+    out["iters_per_s"] = k / max(1e-30, out["time_to_tol_s"])
+    out["F_per_replica_fp64"] = list(fe["FEs"])
+    out["errtot_history"] = hist[::10] + [hist[-1]]
+    out["wall_s"] = time.time() - t_wall
+    print(json.dumps(out))
     return 0
 
 
@@ -578,6 +691,8 @@ def main():
         return run_mixed128(a) if rank == 0 else 0
     if a.workload == "adjoint96":
         return run_adjoint96(a) if rank == 0 else 0
+    if a.workload == "tolerance":
+        return run_tolerance(a) if rank == 0 else 0
     if a.impl == "reference":
         if rank != 0:
             return 0

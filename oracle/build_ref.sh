@@ -3,7 +3,15 @@
 # GPU_kernels.h) from the reference sources for use as a parity oracle and as
 # the reference arm of bench.py.  TEST INFRASTRUCTURE ONLY.
 #
-#   oracle/build_ref.sh STRN [NSTERP] [PRELUDE]
+#   oracle/build_ref.sh STRN [NSTERP] [PRELUDE] [shim]
+#
+# With the fourth argument `shim`, the reference's density.h and
+# GPU_kernels.h are left out: density.h becomes the one-line include of
+# include/density_b200.h (the reference-side binding of this library) and
+# the program links libscft_b200.so, so the reference's own main loop
+# (scft.cu) drives this library's density class.  Output
+# oracle/_ref/scft_shim_<tag>; the PROPS trace (printed from the reference's
+# density.h) is absent from it.
 #
 # The sources are copied into a temporary directory (no reference source is
 # kept or committed) and patched with sed only where the single-process,
@@ -23,15 +31,17 @@
 # Output: oracle/_ref/scft_ref_s<STRN>_n<NSTERP>_p<PRELUDE>
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${SCFT_REFERENCE_DIR:-/root/reference}"
+REF="${SCFT_REFERENCE_DIR:?set SCFT_REFERENCE_DIR to the directory holding the reference scft.cu}"
 STRN="${1:?usage: build_ref.sh STRN [NSTERP] [PRELUDE]}"
 NSTERP="${2:-4000}"
 PRELUDE="${3:-5000}"
+MODE="${4:-ref}"
 TAG="s${STRN}_n${NSTERP}_p${PRELUDE}"
 OUT="$HERE/_ref/scft_ref_${TAG}"
+[ "$MODE" = "shim" ] && OUT="$HERE/_ref/scft_shim_${TAG}"
 SRC="$(mktemp -d)"
 trap 'rm -rf "$SRC"' EXIT
-NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+NVCC="${NVCC:-nvcc}"
 
 if [ ! -f "$REF/scft.cu" ]; then
     echo "reference sources not found at $REF" >&2
@@ -77,7 +87,17 @@ for pat in 'constexpr int strn = STRN;' 'int nsterp=NSTERP;' 'PRELUDE, 1E-4' 'pr
     fi
 done
 
-"$NVCC" -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a \
-    -DSTRN="$STRN" -DNSTERP="$NSTERP" -DPRELUDE="$PRELUDE" \
-    -I"$SRC" -o "$OUT" "$S" -lcufft -w
+if [ "$MODE" = "shim" ]; then
+    ROOT="$(dirname "$HERE")"
+    rm -f "$SRC/GPU_kernels.h"
+    echo '#include "density_b200.h"' > "$D"
+    "$NVCC" -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a \
+        -DSTRN="$STRN" -DNSTERP="$NSTERP" -DPRELUDE="$PRELUDE" \
+        -I"$SRC" -I"$ROOT/include" -o "$OUT" "$S" -L"$ROOT/scft_string_b200" -lscft_b200 \
+        -Xlinker -rpath='$ORIGIN/../../scft_string_b200' -w
+else
+    "$NVCC" -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a \
+        -DSTRN="$STRN" -DNSTERP="$NSTERP" -DPRELUDE="$PRELUDE" \
+        -I"$SRC" -o "$OUT" "$S" -lcufft -w
+fi
 echo "$OUT"

@@ -3,6 +3,7 @@ executable ``scft_b200`` in-tree with nvcc (no JIT cache, no CPU fallback)."""
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -10,7 +11,20 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscft_b200.so")
 EXE = os.path.join(HERE, "scft_b200")
-NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+def _nvcc() -> str:
+    """nvcc from $NVCC, else $CUDA_HOME/bin, else the PATH."""
+    if os.environ.get("NVCC"):
+        return os.environ["NVCC"]
+    home = os.environ.get("CUDA_HOME") or os.environ.get("CUDA_PATH")
+    if home and os.path.exists(os.path.join(home, "bin", "nvcc")):
+        return os.path.join(home, "bin", "nvcc")
+    found = shutil.which("nvcc")
+    if not found:
+        raise RuntimeError("nvcc not found: set NVCC or CUDA_HOME, or put nvcc on the PATH")
+    return found
+
+
+NVCC = _nvcc()
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu", "noalloc.cu",
               "density_ckpt.cu", "reg64.cu"]

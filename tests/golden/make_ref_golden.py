@@ -30,7 +30,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
 from cases import CASES  # noqa: E402
-from scft_string_b200.configs import PLAIN_32, fields, input_dat, win_text  # noqa: E402
+from scft_string_b200.configs import (ADJOINT_96, PLAIN_32, STRING_64, fields, hex_fields, input_dat,  # noqa: E402
+                                      win_text)
 
 PRELUDE = 5000
 
@@ -41,18 +42,34 @@ def all_cases():
     c1["nsterp"] = 200
     c1["trace_only"] = True
     out["plain32_c1"] = c1
+    # the benchmarked string: 16 replicas of 64^3, N = 128; W+ prelude and the
+    # first five string iterations (FreeE at k = 0 and at the last one)
+    c2 = dict(STRING_64)
+    c2["nsterp"] = 5
+    c2["trace_only"] = True
+    out["string64_c2"] = c2
+    # the 64x64x96, N = 160 adjoint workload from its hexagonal start: a short
+    # W+ prelude (20 props) and two iterations of the plain method
+    c4 = dict(ADJOINT_96)
+    c4.update(nsterp=2, prelude=20, trace_only=True, start="hex")
+    out["adjoint96_c4"] = c4
     return out
 
 
+def case_fields(c):
+    return hex_fields(c) if c.get("start") == "hex" else fields(c)
+
+
 def binary(c):
-    return os.path.join(ROOT, "oracle", "_ref", f"scft_ref_s{c['strn']}_n{c['nsterp']}_p{PRELUDE}")
+    return os.path.join(ROOT, "oracle", "_ref",
+                        f"scft_ref_s{c['strn']}_n{c['nsterp']}_p{c.get('prelude', PRELUDE)}")
 
 
 def build():
     for name, c in all_cases().items():
         if not os.path.exists(binary(c)):
             subprocess.run([os.path.join(ROOT, "oracle", "build_ref.sh"), str(c["strn"]),
-                            str(c["nsterp"]), str(PRELUDE)], check=True)
+                            str(c["nsterp"]), str(c.get("prelude", PRELUDE))], check=True)
         print(name, binary(c))
 
 
@@ -72,7 +89,7 @@ def parse_trace(text):
 
 
 def run_case(name, c, outdir):
-    wm, wp = fields(c)
+    wm, wp = case_fields(c)
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "input.dat"), "w") as fh:
             fh.write(input_dat(c))

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from scft_string_b200.configs import fields
+from scft_string_b200.configs import fields, hex_fields
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -23,7 +23,7 @@ def load_fixture(name):
 
 def initial_fields(c):
     """(W- rows, W+ rows, springsteps) after the reference's win-file read."""
-    wm, wp = fields(c)
+    wm, wp = hex_fields(c) if c.get("start") == "hex" else fields(c)
     wm, wp = wm.copy(), wp.copy()
     missing = set(c.get("missing", ()))
     springsteps, cpto0 = 0, False

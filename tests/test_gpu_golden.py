@@ -17,7 +17,7 @@ def run_gpu(c, batched=True, precision="fp64"):
     ctx = S.StringSolver(c, precision=precision, batched=batched, springsteps=springsteps)
     for ii in range(c["strn"]):
         ctx.set_fields(ii, wm[ii], wp[ii])
-    ctx.solve_field0_all(5000, 1e-4)
+    ctx.solve_field0_all(c.get("prelude", 5000), 1e-4)
     k, recs, errs, errs3 = ctx.solve_field(c["nsterp"])
     fe = ctx.free_energy()
     return ctx, k, recs, errs, errs3, fe
@@ -60,3 +60,33 @@ def test_fp64_plain32_c1_trace(built_lib):
     _, lnQ, phis = ctx.get_conc(0)
     assert abs(lnQ - ref["props"][-1, 2]) <= TOL * abs(ref["props"][-1, 2])
     assert np.allclose(phis, ref["props"][-1, 3:8], rtol=TOL)
+
+
+@pytest.mark.parametrize("name", ["string64_c2", "adjoint96_c4"])
+def test_fp64_benchmark_configs_match_reference_trace(built_lib, name):
+    """The benchmarked 16-replica 64^3 string (W+ prelude, five string
+    iterations, FreeE at k = 0 and k = 4) and the 64x64x96, N = 160
+    workload from its hexagonal start (20 prelude props, two iterations):
+    the number of props calls, the per-iteration errs/errs3, the final FreeE
+    and the last props call's lnQ and phis against the reference program's
+    own run."""
+    try:
+        fx = load_fixture(name)
+    except FileNotFoundError:
+        pytest.skip(f"fixture ref_{name} not recorded")
+    ref = ref_trace(fx)
+    c = fx["params"]
+    ctx, k, recs, errs, errs3, fe = run_gpu(c, batched=True)
+    assert k == len(ref["errs"])
+    assert ctx.stats()["props_calls"] == ref["nprops"]
+    assert np.allclose(errs, ref["errs"], rtol=TOL, atol=1e-300)
+    assert np.allclose(errs3, ref["errs3"], rtol=TOL, atol=1e-300)
+    last = ref["final_freee"]
+    assert np.allclose(fe["FEs0"], last[:, 1], rtol=TOL)
+    assert np.allclose(fe["FEs1"], last[:, 2], rtol=TOL, atol=1e-12)
+    assert np.allclose(fe["phctot"], last[:, 3], rtol=TOL)
+    for ii in range(c["strn"]):
+        _, lnQ, phis = ctx.get_conc(ii)
+        assert abs(-lnQ - last[ii, 1]) <= TOL * max(1.0, abs(last[ii, 1]))
+    assert abs(lnQ - ref["props"][-1, 2]) <= TOL * max(1.0, abs(ref["props"][-1, 2]))
+    assert np.allclose(phis, ref["props"][-1, 3:8], rtol=TOL, atol=1e-14)

@@ -14,8 +14,8 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("SCFT_REFERENCE_DIR", "/root/reference")
-NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+REF = os.environ.get("SCFT_REFERENCE_DIR", "")
+NVCC = os.environ.get("NVCC") or shutil.which("nvcc") or "nvcc"
 PKG = os.path.join(ROOT, "scft_string_b200")
 
 MPI_STUB = """#pragma once

@@ -43,6 +43,7 @@ struct PropsArgs {
     int *err;               // device error word (launch-geometry / plan errors)
     int slot0;              // first slot of this launch within the spectra tensor map
     T *jtab;                // [slot][M]  junction-step E4 (continuous A fraction only)
+    int *sync;              // claim and completion counters of the persistent step kernel (reg64.cu)
 };
 
 struct PropsLaunch {
@@ -61,6 +62,8 @@ struct PropsLaunch {
     int pencil_tma_smem_wide;
     const CUtensorMap *tmap_wide;  // the same spectra with the wide tile box
     int reg;         // 64^3 FP32: register-resident step kernels (reg64.cu) instead of the shared-memory ones
+    int persist;     // with reg: one persistent launch per contour step instead of four
+    int step_grid;   // CTAs of that launch
 };
 
 // register-resident 64^3 FP32 step kernels (reg64.cu)
@@ -69,6 +72,9 @@ int reg64_set_smem();
 void reg64_combine(const PropsArgs<float> &a, int nslots, int s, int mode, cudaStream_t st);
 void reg64_mid(const PropsArgs<float> &a, int nslots, int s, cudaStream_t st);
 void reg64_pencil(const PropsArgs<float> &a, int nslots, int both, cudaStream_t st);
+int reg64_sync_ints(int Ns, int nslots);
+int reg64_step_grid();
+void reg64_step(const PropsArgs<float> &a, int nslots, int s, int grid, cudaStream_t st);
 
 void pf_smem_bytes(int id, int fp32, int &mid, int &comb);
 

@@ -894,18 +894,31 @@ int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cud
     const Geo &g = a.g;
     dim3 gs(g.m0, 2, nslots), gp(g.ncol_tiles, 2, nslots);
     k_prepare<T><<<dim3(L.ew_blocks, nslots), 256, 0, st>>>(a);
-    launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
-    for (int s = 0; s < g.Ns; s++) {
-        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 1, st);
-        launch_mid<T, MT, F0, F1, F2>(a, L, gs, s, st);
-        launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 0, st);
-        launch_combine<T, MT, F0, F1, F2>(a, L, gs, s, 0, st);
+    int n = 6;
+    if constexpr (kReg64<T, F0, F1, F2>) {
+        if (L.reg && L.persist) {
+            // one persistent launch per contour step (reg64.cu); its counters start at zero
+            cudaMemsetAsync(a.sync, 0, sizeof(int) * reg64_sync_ints(g.Ns, nslots), st);
+            launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
+            for (int s = 0; s < g.Ns; s++) reg64_step(a, nslots, s, L.step_grid, st);
+            n += g.Ns;
+        }
+    }
+    if (n == 6) {
+        launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
+        for (int s = 0; s < g.Ns; s++) {
+            launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 1, st);
+            launch_mid<T, MT, F0, F1, F2>(a, L, gs, s, st);
+            launch_pencil<T, MT, F0, F1, F2>(a, L, gp, 0, st);
+            launch_combine<T, MT, F0, F1, F2>(a, L, gs, s, 0, st);
+        }
+        n += 4 * g.Ns;
     }
     k_qsum<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
     k_qfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
     k_density<T><<<dim3(L.red_blocks, nslots), 256, 0, st>>>(a);
     k_dfinal<T><<<nslots, 32, 0, st>>>(a, L.red_blocks);
-    return 4 * g.Ns + 6;
+    return n;
 }
 
 // one contour step s of slot 0 starting from the propagator store slice s

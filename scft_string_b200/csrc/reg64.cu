@@ -71,14 +71,12 @@ __device__ __forceinline__ void slab_forward(float *R, float2 *out, int lane, fl
 }
 
 // ---------------------------------------------------------------- pencil
-// both != 0: spectrum A times K2 and spectrum B times K1; else A with K2 only
-// (Mult_self, GPU_kernels.h:175-181; factors Prepare_dev_expKsq2_expKsq,
-// GPU_kernels.h:207-213, from the replica's separable per-axis table)
-__global__ void __launch_bounds__(kPencilThreads) k_pencil_r(PropsArgs<float> a, int both)
+// Column c of spectrum A (times K2) and, when both != 0, of spectrum B (times
+// K1) of (slot, fld) (Mult_self, GPU_kernels.h:175-181; factors
+// Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213, from the replica's
+// separable per-axis table).
+__device__ __forceinline__ void pencil_column(const PropsArgs<float> &a, int both, int slot, int fld, int c)
 {
-    const int c = blockIdx.x * kPencilThreads + threadIdx.x;
-    const int fld = blockIdx.y, slot = blockIdx.z;
-    if (c >= kPlane) return;
     const int ky = c / kMK, kz = c - ky * kMK;
     const float *kf = a.kfac + (size_t)a.slot_rep[slot] * a.kf_stride;  // x (64) | y (64) | z (33)
     const float colf = kf[64 + ky] * kf[128 + kz];
@@ -89,7 +87,7 @@ __global__ void __launch_bounds__(kPencilThreads) k_pencil_r(PropsArgs<float> a,
         float2 *sp = spec + (size_t)pass * kMk + c;
         float2 v[64];
 #pragma unroll
-        for (int x = 0; x < 64; x++) v[x] = sp[(size_t)x * kPlane];
+        for (int x = 0; x < 64; x++) v[x] = ld_shared_gm(sp + (size_t)x * kPlane);
         fft64<-1>(v);  // bin kx in v[perm(kx)]
 #pragma unroll
         for (int kx = 0; kx < 64; kx++) {
@@ -105,12 +103,11 @@ __global__ void __launch_bounds__(kPencilThreads) k_pencil_r(PropsArgs<float> a,
 }
 
 // ---------------------------------------------------------------- mid
-__global__ void __launch_bounds__(32 * kWPB) k_mid_r(PropsArgs<float> a, int s)
+// slab x of (slot, fld) by one warp with tile R: inverse slab of the full step
+// -> P = E2 qs1; inverse slab of the half step, times E2, forward slab
+__device__ __forceinline__ void mid_slab(const PropsArgs<float> &a, int s, int slot, int fld, int x, float *R,
+                                         int lane)
 {
-    extern __shared__ __align__(16) float smem_r[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x = blockIdx.x * kWPB + warp, fld = blockIdx.y, slot = blockIdx.z;
-    float *R = smem_r + warp * kTileFloats;
     const Geo &g = a.g;
     const size_t slab_r = (size_t)x * 4096;
     const float *E = eptr(a, slot, esel(g, fld, s)) + slab_r;
@@ -144,12 +141,9 @@ __global__ void __launch_bounds__(32 * kWPB) k_mid_r(PropsArgs<float> a, int s)
 // mode 1: q(s+1) = 1 (Array_set_value, density.h:368-369; called with s = -1);
 // mode 2: q(s+1) is taken from the propagator store.
 // Then starts step s+1 when s+1 < Ns.
-__global__ void __launch_bounds__(32 * kWPB) k_combine_r(PropsArgs<float> a, int s, int mode)
+__device__ __forceinline__ void combine_slab(const PropsArgs<float> &a, int s, int mode, int slot, int fld, int x,
+                                             float *R, int lane)
 {
-    extern __shared__ __align__(16) float smem_r[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x = blockIdx.x * kWPB + warp, fld = blockIdx.y, slot = blockIdx.z;
-    float *R = smem_r + warp * kTileFloats;
     const Geo &g = a.g;
     const size_t slab_r = (size_t)x * 4096;
     float2 *specA = reinterpret_cast<float2 *>(a.spec) + ((size_t)slot * 2 + fld) * 2 * kMk;
@@ -167,7 +161,7 @@ __global__ void __launch_bounds__(32 * kWPB) k_combine_r(PropsArgs<float> a, int
             float2 *cp = reinterpret_cast<float2 *>(R + y * kRowPitch + z);
             const float2 c = *cp;
             const float2 e = *reinterpret_cast<const float2 *>(E + y * 64 + z);
-            const float2 p = *reinterpret_cast<const float2 *>(P + y * 64 + z);
+            const float2 p = ld_shared_gm(reinterpret_cast<const float2 *>(P + y * 64 + z));
             const float2 q = make_float2((c.x * e.x * 4.0f - p.x) / 3.0f, (c.y * e.y * 4.0f - p.y) / 3.0f);
             *reinterpret_cast<float2 *>(qn + y * 64 + z) = q;
             *cp = q;
@@ -195,7 +189,7 @@ __global__ void __launch_bounds__(32 * kWPB) k_combine_r(PropsArgs<float> a, int
         *cp = make_float2(c.x * e.x, c.y * e.y);
     }
     slab_forward(R, specA + (size_t)x * kPlane, lane, v);
-    // full step input E2' q' (q' re-read from the propagator store written above)
+    // full step input E2' q' (q' re-read from the propagator store: this lane wrote it above)
 #pragma unroll 4
     for (int y = 0; y < 64; y++) {
         const float2 q = *reinterpret_cast<const float2 *>(qn + y * 64 + z);
@@ -203,6 +197,104 @@ __global__ void __launch_bounds__(32 * kWPB) k_combine_r(PropsArgs<float> a, int
         *reinterpret_cast<float2 *>(R + y * kRowPitch + z) = make_float2(q.x * (e.x * e.x), q.y * (e.y * e.y));
     }
     slab_forward(R, specB + (size_t)x * kPlane, lane, v);
+}
+
+__global__ void __launch_bounds__(kPencilThreads) k_pencil_r(PropsArgs<float> a, int both)
+{
+    const int c = blockIdx.x * kPencilThreads + threadIdx.x;
+    if (c < kPlane) pencil_column(a, both, blockIdx.z, blockIdx.y, c);
+}
+
+__global__ void __launch_bounds__(32 * kWPB) k_mid_r(PropsArgs<float> a, int s)
+{
+    extern __shared__ __align__(16) float smem_r[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    mid_slab(a, s, blockIdx.z, blockIdx.y, blockIdx.x * kWPB + warp, smem_r + warp * kTileFloats, lane);
+}
+
+__global__ void __launch_bounds__(32 * kWPB) k_combine_r(PropsArgs<float> a, int s, int mode)
+{
+    extern __shared__ __align__(16) float smem_r[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    combine_slab(a, s, mode, blockIdx.z, blockIdx.y, blockIdx.x * kWPB + warp, smem_r + warp * kTileFloats, lane);
+}
+
+// ---------------------------------------------------------------- one launch per contour step
+// A persistent kernel runs the whole step s of every slot: CTAs claim work
+// items from a counter in a fixed order -- all pencil(both) column blocks,
+// then all mid slab quads, all pencil(A) column blocks, all combine slab
+// quads, each phase ordered by (slot, field) -- and an item waits only for
+// the items of the previous phase of its own (slot, field).  Items are
+// claimed in order by running CTAs, so whatever an item waits for has been
+// claimed by a CTA that is running or done: no residency assumption is
+// needed.  Completion counters are cumulative over the steps of a props
+// round (phase p of (slot, field) has n_p (s+1) items done after step s) and
+// are zeroed with the claim counters when the round starts.  Every wait is
+// bounded (kStepSpin polls); one that gives up records error 3 and ends the
+// kernel, so a lost item cannot hang the GPU.  Data another CTA of the same
+// launch wrote (spectra, P) is read through L2 (ld_shared_gm).
+constexpr int kColBlocks = (kPlane + kPencilThreads - 1) / kPencilThreads;  // 17
+constexpr int kSlabQuads = 64 / kWPB;                                       // 16
+constexpr uint32_t kStepSpin = 1u << 22;
+
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(32 * kWPB) k_step_r(PropsArgs<float> a, int s, int nslots)
+{
+    extern __shared__ __align__(16) float smem_r[];
+    __shared__ int item_sh, ok_sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = 2 * nslots;  // (slot, field) groups
+    const int per[4] = {kColBlocks, kSlabQuads, kColBlocks, kSlabQuads};
+    const int total = G * (2 * kColBlocks + 2 * kSlabQuads);
+    int *claim = a.sync + s;           // this step's claim counter
+    int *done = a.sync + a.g.Ns;       // [phase][group] completion counters
+    for (;;) {
+        if (threadIdx.x == 0) item_sh = atomicAdd(claim, 1);
+        __syncthreads();
+        int it = item_sh;
+        if (it >= total) break;
+        int phase = 0;
+        while (it >= G * per[phase]) {
+            it -= G * per[phase];
+            phase++;
+        }
+        const int group = it / per[phase], unit = it - group * per[phase];
+        const int slot = group >> 1, fld = group & 1;
+        if (phase > 0) {
+            if (threadIdx.x == 0) {
+                const int need = per[phase - 1] * (s + 1);
+                const int *cnt = done + (phase - 1) * G + group;
+                uint32_t i = 0;
+                while (ld_acquire(cnt) < need && i < kStepSpin) {
+                    __nanosleep(32);
+                    i++;
+                }
+                ok_sh = i < kStepSpin;
+                if (!ok_sh) *a.err = 3;
+            }
+            __syncthreads();
+            if (!ok_sh) return;
+        }
+        if (phase == 0 || phase == 2) {
+            const int c = unit * kPencilThreads + threadIdx.x;
+            if (c < kPlane) pencil_column(a, phase == 0, slot, fld, c);
+        } else if (phase == 1) {
+            mid_slab(a, s, slot, fld, unit * kWPB + warp, smem_r + warp * kTileFloats, lane);
+        } else {
+            combine_slab(a, s, 0, slot, fld, unit * kWPB + warp, smem_r + warp * kTileFloats, lane);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done + phase * G + group, 1);
+        }
+    }
 }
 
 constexpr int kSlabSmem = kWPB * kTileFloats * (int)sizeof(float);
@@ -215,7 +307,25 @@ int reg64_set_smem()
 {
     cudaError_t e1 = cudaFuncSetAttribute(k_mid_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
     cudaError_t e2 = cudaFuncSetAttribute(k_combine_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
-    return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
+    cudaError_t e3 = cudaFuncSetAttribute(k_step_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
+    return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : 1;
+}
+
+int reg64_sync_ints(int Ns, int nslots) { return Ns + 4 * 2 * nslots; }
+
+int reg64_step_grid()
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_r, 32 * kWPB, kSlabSmem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return sms * per_sm;
+}
+
+void reg64_step(const PropsArgs<float> &a, int nslots, int s, int grid, cudaStream_t st)
+{
+    k_step_r<<<grid, 32 * kWPB, kSlabSmem, st>>>(a, s, nslots);
 }
 
 void reg64_combine(const PropsArgs<float> &a, int nslots, int s, int mode, cudaStream_t st)

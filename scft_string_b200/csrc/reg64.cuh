@@ -95,6 +95,17 @@ constexpr TwTable kTw = make_table();
 
 SCFT_HD constexpr int perm(int k) { return (k >> 3) + 8 * (k & 7); }
 
+// load of data that other CTAs of the same launch may have written (the
+// persistent step kernel): served from L2, never from a stale L1 line
+SCFT_HD float2 ld_shared_gm(const float2 *p)
+{
+#ifdef __CUDA_ARCH__
+    return __ldcg(p);
+#else
+    return *p;
+#endif
+}
+
 SCFT_HD float2 cadd2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 SCFT_HD float2 csub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 // a * exp(SIGN 2 pi i t/64)
@@ -240,12 +251,12 @@ SCFT_HD void iy(const float2 *in, int kz, float2 *v, float2 *T)
     if (kz == 0) {
 #pragma unroll
         for (int k = 0; k < 64; k++) {
-            const float2 a = in[k * kMK], h = in[k * kMK + 32];
+            const float2 a = ld_shared_gm(in + k * kMK), h = ld_shared_gm(in + k * kMK + 32);
             v[k] = make_float2(a.x - h.y, a.y + h.x);
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < 64; k++) v[k] = in[k * kMK + kz];
+        for (int k = 0; k < 64; k++) v[k] = ld_shared_gm(in + k * kMK + kz);
     }
     fft64<+1>(v);
 #pragma unroll

@@ -79,6 +79,8 @@ struct scft_ctx {
     double *partials = nullptr, *redout = nullptr;
     int npart_stride = 0, nred_rows = 0;
     int *rep_dev = nullptr, *err = nullptr;
+    int *sync = nullptr;     // counters of the persistent step kernel, one block per slot group
+    int sync_stride = 0;
     std::vector<double> Dr;  // box of every replica (3 per replica); p.D is the last common box
     int kf_n = 0;            // diffusion factors per replica (m0 + m1 + mk2)
     void *jtab = nullptr;  // junction-step E table per slot (continuous A fraction)
@@ -162,6 +164,7 @@ PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
     a.alpha = ctx->p.alpha;
     a.ens = ctx->p.ens;
     a.err = ctx->err;
+    a.sync = ctx->sync;
     a.slot0 = 0;
     a.jtab = (T *)ctx->jtab;
     return a;
@@ -181,6 +184,7 @@ PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0)
     a.partials += (size_t)s0 * ctx->npart_stride;
     a.slot0 = s0;
     if (a.jtab) a.jtab += (size_t)s0 * M;
+    if (a.sync && s0 > 0) a.sync += ctx->sync_stride;  // the second slot group's counters
     return a;
 }
 
@@ -293,7 +297,7 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
                 if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
             }
             CK(cudaGraphLaunch(ctx->graphs[key], ctx->st));
-            launches += (4 * ctx->g.Ns + 6) * ng;
+            launches += ((ctx->L.reg && ctx->L.persist ? 1 : 4) * ctx->g.Ns + 6) * ng;
         } else {
             launches += launch();
         }
@@ -574,7 +578,7 @@ void scft_destroy(scft_ctx *ctx)
     void *ptrs[] = {ctx->W, ctx->conc, ctx->DEV, ctx->dWda, ctx->rs, ctx->partials, ctx->redout,
                     ctx->rep_dev, ctx->err, ctx->etab, ctx->hist, ctx->spec, ctx->pbuf, ctx->tw,
                     ctx->kfac, ctx->knots, ctx->st_S4, ctx->st_S2, ctx->st_S4p, ctx->st_part,
-                    ctx->st_out, ctx->and_X, ctx->and_D, ctx->ck_mem, ctx->jtab, ctx->jd_rbuf};
+                    ctx->st_out, ctx->and_X, ctx->and_D, ctx->ck_mem, ctx->jtab, ctx->jd_rbuf, ctx->sync};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : ctx->tev)
@@ -732,6 +736,10 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMalloc(&ctx->hist, ctx->nostore ? T * 2 * M : T * 2 * M * (size_t)(g.Ns + 1) * S));
         CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
         CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
+        if (L.reg) {
+            ctx->sync_stride = reg64_sync_ints(g.Ns, (int)S);
+            CKC(cudaMalloc(&ctx->sync, sizeof(int) * 2 * (size_t)ctx->sync_stride));
+        }
         CKC(cudaMalloc(&ctx->tw, twb.size()));
         // one block of diffusion factors per replica (every replica may own its box)
         ctx->kf_n = g.m0 + g.m1 + g.mk2;
@@ -791,6 +799,14 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
             ctx->lasterr = "cudaFuncSetAttribute(max dynamic shared memory) failed";
             rc = SCFT_CUDA_ERROR;
             goto done;
+        }
+        // register kernels: one persistent launch per contour step unless SCFT_NO_PERSIST=1
+        // (scft_autotune compares it with four launches per step)
+        L.persist = 0;
+        if (L.reg) {
+            L.step_grid = reg64_step_grid();
+            L.persist = 1;
+            if (const char *ev = getenv("SCFT_NO_PERSIST")) L.persist = ev[0] == '1' ? 0 : 1;
         }
         ctx->doiis.assign(ctx->strn, 1);  // one process owns every replica (scft.cu:952-975)
         ctx->graphs.assign((size_t)(R + 1) * (S + 1) + 1, nullptr);
@@ -2214,14 +2230,20 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
     };
     double best = 0;
     int best_g = 1, best_w = 0;
-    const int nw = (ctx->L.tmap_wide && !ctx->L.reg) ? 2 : 1;  // the register kernels have no pencil tiles
+    // second axis: x-pencil tile width, or -- with the register kernels, which
+    // have no pencil tiles -- one persistent launch per step against four
+    const bool reg = ctx->L.reg != 0;
+    const int nw = reg ? 2 : (ctx->L.tmap_wide ? 2 : 1);
     for (int c = 0; c < 4; c++) {
         const int ng = 1 + (c & 1), wide = c >> 1;
         if (times_ms) times_ms[c] = -1;
         if (wide >= nw) continue;
         drop_graphs();
         ctx->ngroups = ng;
-        ctx->L.ptile_wide = wide;
+        if (reg)
+            ctx->L.persist = wide;
+        else
+            ctx->L.ptile_wide = wide;
         scft_status s = props_list(ctx, all);
         if (s != SCFT_OK) return s;
         double t = 1e300;
@@ -2240,7 +2262,10 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
     }
     drop_graphs();
     ctx->ngroups = best_g;
-    ctx->L.ptile_wide = best_w;
+    if (reg)
+        ctx->L.persist = best_w;
+    else
+        ctx->L.ptile_wide = best_w;
     ctx->stats = keep;
     if (groups_out) *groups_out = best_g;
     if (wide_out) *wide_out = best_w;

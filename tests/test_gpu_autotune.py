@@ -30,3 +30,42 @@ def test_autotune_schedules_give_identical_densities(built_lib, precision):
         np.testing.assert_array_equal(conc, ref[ii][0])
         assert lnq == ref[ii][1]
     print(precision, "schedule", groups, wide, "round ms", t)
+
+
+def test_persistent_step_launch_matches_four_launches(built_lib, monkeypatch):
+    """64^3 FP32 runs the register-resident step kernels; one persistent
+    launch per contour step (work items claimed in order, waits bounded) and
+    four launches per step run the same arithmetic, so the densities and lnQ
+    of a props round agree bit for bit, and the autotuner's four schedules
+    leave them unchanged."""
+    c = dict(STRING_64, N=40, strn=4)
+    wm, wp = fields(c)
+
+    def run(no_persist):
+        if no_persist:
+            monkeypatch.setenv("SCFT_NO_PERSIST", "1")
+        else:
+            monkeypatch.delenv("SCFT_NO_PERSIST", raising=False)
+        ctx = S.StringSolver(c, precision="fp32")
+        for ii in range(c["strn"]):
+            ctx.set_fields(ii, wm[ii], wp[ii])
+        ctx.solve_field0_all(2, 0.0)  # one batched props round of every replica (then a W+ update)
+        return ctx, [ctx.get_conc(ii) for ii in range(c["strn"])]
+
+    ctx, persistent = run(False)
+    launches = ctx.stats()["kernel_launches"]
+    ctx4, four = run(True)
+    assert ctx4.stats()["kernel_launches"] > 3 * launches  # 4 N + 6 against N + 6 per round
+    for (ca, qa, pa), (cb, qb, pb) in zip(persistent, four):
+        np.testing.assert_array_equal(ca, cb)
+        assert qa == qb
+    ref = []
+    for ii in range(c["strn"]):  # densities at the fields after the W+ update
+        ctx.props(ii)
+        ref.append(ctx.get_conc(ii)[0])
+    groups, persist, t = ctx.autotune()
+    assert groups in (1, 2) and persist in (0, 1) and all(v > 0 for v in t), t
+    for ii in range(c["strn"]):
+        conc, lnq, _ = ctx.get_conc(ii)
+        np.testing.assert_array_equal(conc, ref[ii])
+    print("round ms (g1 four, g2 four, g1 persistent, g2 persistent)", t)

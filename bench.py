@@ -9,6 +9,12 @@ of every replica, residuals, spline tangent projection, mixing and equal-arc
 redistribution.  Each rank runs its own copy of the string (replicas only, no
 collective on the data path); value = steps of all ranks / max-rank device time.
 
+The default timed arm is the batched FP64 path: the reference's arithmetic,
+so its ratio to the reference arm compares like with like.  The batched FP32
+path (the metric's "fused FP32") and the plain FP64 path (one replica at a
+time) are timed on the same iterations and reported beside it, with the FP32
+path's errors against FP64 at identical fields.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp64] [--plain]
 """
@@ -34,7 +40,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["fp32", "fp64"],
+                    help="propagator arithmetic of the timed arm (fp64: the reference's; the other precision "
+                         "and plain FP64 run on the same window beside it)")
     ap.add_argument("--plain", action="store_true", help="one replica at a time")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -674,6 +682,21 @@ def run_ours(a, cfg, rank, world, dev):
                              errtot_last=rr[-1]["errtot"])
             c.close()
         out["cmp"] = res
+        # FP32 propagator against FP64 at identical fields: the state at k = W
+        one64 = S.StringSolver(dict(cfg, strn=1), precision="fp64", device=dev)
+        one32 = S.StringSolver(dict(cfg, strn=1), precision="fp32", device=dev)
+        dF, dq, dr = [], [], []
+        for ii in range(strn):
+            w = np.ascontiguousarray(host_w[ii])
+            F64, q64, r64 = f_per_chain(one64, cfg, w)
+            F32, q32, r32 = f_per_chain(one32, cfg, w)
+            dF.append(abs(F32 - F64))
+            dq.append(abs(q32 - q64) / max(1e-300, abs(q64)))
+            dr.append(float(np.abs(r32 - r64).max()))
+        one64.close()
+        one32.close()
+        out["fp32_err"] = {"at": f"fields of every replica at k={W0}",
+                           "F_per_chain": dF, "lnQ_rel": dq, "rhoA_maxabs": dr}
     D.finalize(world)
     return out
 
@@ -781,6 +804,8 @@ def main():
             line["fp32_batched_vs_fp64_plain"] = c["fp32_batched"]["iters_per_s"] / c["fp64_plain"]["iters_per_s"]
         if a.precision == "fp64" and not a.plain and "fp64_plain" in c:
             line["fp64_batched_vs_fp64_plain"] = value / c["fp64_plain"]["iters_per_s"]
+    if "fp32_err" in r:
+        line["fp32_vs_fp64_at_identical_fields"] = r["fp32_err"]
     if world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(cfg, props_per_iter)
     print(json.dumps(line))

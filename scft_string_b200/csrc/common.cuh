@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 namespace scft {
 
 template <typename T>
@@ -61,5 +63,24 @@ struct Geo {
     int jon, jq, jqd;
     double theta;
 };
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`, never
+// lowers it.  The limit belongs to the kernel, not to a context: the
+// runtime-shaped kernels serve every context of any grid, so a context that
+// set it to its own (smaller) need would make the launches of an earlier,
+// larger context fail.  Serialised, so concurrent context creation keeps
+// the largest value.
+template <typename F>
+inline cudaError_t raise_dyn_smem(F *fn, int bytes)
+{
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, reinterpret_cast<const void *>(fn));
+    if (e != cudaSuccess) return e;
+    if (at.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes);
+}
 
 }  // namespace scft

@@ -192,6 +192,9 @@ extern "C" scft_status scft_do_step_noalloc(const int *m, const double *D, int N
     // whose store holds only slices s and s+1: its geometry counts contour
     // steps from s, so n1 and n2 shrink by s and each step still picks the E
     // table of its absolute index
+    // the runtime-shaped kernels' shared-memory limits are raised to this
+    // grid's need if they are below it (host-side attribute, no allocation)
+    if (set_props_smem<double>(L) != 0) return SCFT_CUDA_ERROR;
     launch_prepare<double>(a, L, st);
     PropsArgs<double> seg = a;
     seg.g.Ns = 1;

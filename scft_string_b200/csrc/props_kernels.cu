@@ -958,21 +958,19 @@ int launch_chain_mt(const PropsArgs<T> &a, const PropsLaunch &L, int first_mode,
 template <typename T, int MT, int F0, int F1, int F2>
 int set_smem_mt(const PropsLaunch &L)
 {
-    cudaError_t e1 = cudaFuncSetAttribute(k_combine<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
-    cudaError_t e2 = cudaFuncSetAttribute(k_mid<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.slab_smem);
-    cudaError_t e3 = cudaFuncSetAttribute(k_pencil<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_smem);
+    cudaError_t e1 = raise_dyn_smem(k_combine<T, MT, F0, F1, F2>, L.slab_smem);
+    cudaError_t e2 = raise_dyn_smem(k_mid<T, MT, F0, F1, F2>, L.slab_smem);
+    cudaError_t e3 = raise_dyn_smem(k_pencil<T, MT, F0, F1, F2>, L.pencil_smem);
     cudaError_t e4 = cudaSuccess, e5 = cudaSuccess;
     if constexpr (F1 != 0) {
         if (L.tma_pencil) {
-            e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2, kTile<T>::value>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem);
+            e4 = raise_dyn_smem(k_pencil_tma<T, MT, F0, F1, F2, kTile<T>::value>, L.pencil_tma_smem);
             if (e4 == cudaSuccess && L.tmap_wide)
-                e4 = cudaFuncSetAttribute(k_pencil_tma<T, MT, F0, F1, F2, 2 * kTile<T>::value>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, L.pencil_tma_smem_wide);
+                e4 = raise_dyn_smem(k_pencil_tma<T, MT, F0, F1, F2, 2 * kTile<T>::value>, L.pencil_tma_smem_wide);
         }
         if (e4 == cudaSuccess && L.pf) {
-            e4 = cudaFuncSetAttribute(k_combine_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.combine_pf_smem);
-            e5 = cudaFuncSetAttribute(k_mid_pf<T, MT, F0, F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.mid_pf_smem);
+            e4 = raise_dyn_smem(k_combine_pf<T, MT, F0, F1, F2>, L.combine_pf_smem);
+            e5 = raise_dyn_smem(k_mid_pf<T, MT, F0, F1, F2>, L.mid_pf_smem);
         }
     }
     int e6 = 0;

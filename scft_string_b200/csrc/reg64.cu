@@ -44,9 +44,13 @@ __device__ __forceinline__ const float *eptr(const PropsArgs<float> &a, int slot
     return sel == 2 ? a.jtab + (size_t)slot * kM : a.etab + ((size_t)slot * 2 + sel) * kM;
 }
 
-// inverse slab transform of the spectrum plane `in` into the real tile R
-__device__ __forceinline__ void slab_inverse(const float2 *in, float *R, int lane, float2 *v)
+// inverse slab transform of the spectrum plane `in` into the real tile R.
+// The slab transforms are kept out of line: every kernel calls them two or
+// three times, and inlined copies of their unrolled 64-point transforms
+// overflow the instruction cache.
+__device__ __noinline__ void slab_inverse(const float2 *in, float *R, int lane)
 {
+    float2 v[64];
     float2 *T = reinterpret_cast<float2 *>(R);
     __syncwarp();
     iy(in, lane, v, T);
@@ -58,8 +62,9 @@ __device__ __forceinline__ void slab_inverse(const float2 *in, float *R, int lan
 }
 
 // forward slab transform of the real tile R into the spectrum plane `out`
-__device__ __forceinline__ void slab_forward(float *R, float2 *out, int lane, float2 *v)
+__device__ __noinline__ void slab_forward(float *R, float2 *out, int lane)
 {
+    float2 v[64];
     float2 *T = reinterpret_cast<float2 *>(R);
     __syncwarp();
     fz_load(R, lane, v);
@@ -115,9 +120,8 @@ __device__ __forceinline__ void mid_slab(const PropsArgs<float> &a, int s, int s
     float2 *specB = specA + kMk;
     float *P = a.pbuf + ((size_t)slot * 2 + fld) * kM + slab_r;
     const int z = 2 * lane;
-    float2 v[64];
     // full step: P = E2 * qs1
-    slab_inverse(specB + (size_t)x * kPlane, R, lane, v);
+    slab_inverse(specB + (size_t)x * kPlane, R, lane);
 #pragma unroll 4
     for (int y = 0; y < 64; y++) {
         const float2 c = *reinterpret_cast<const float2 *>(R + y * kRowPitch + z);
@@ -125,7 +129,7 @@ __device__ __forceinline__ void mid_slab(const PropsArgs<float> &a, int s, int s
         *reinterpret_cast<float2 *>(P + y * 64 + z) = make_float2(c.x * (e.x * e.x), c.y * (e.y * e.y));
     }
     // second half step input: E2 * (first half step)
-    slab_inverse(specA + (size_t)x * kPlane, R, lane, v);
+    slab_inverse(specA + (size_t)x * kPlane, R, lane);
 #pragma unroll 4
     for (int y = 0; y < 64; y++) {
         float2 *cp = reinterpret_cast<float2 *>(R + y * kRowPitch + z);
@@ -133,7 +137,7 @@ __device__ __forceinline__ void mid_slab(const PropsArgs<float> &a, int s, int s
         const float2 e = *reinterpret_cast<const float2 *>(E + y * 64 + z);
         *cp = make_float2(c.x * (e.x * e.x), c.y * (e.y * e.y));
     }
-    slab_forward(R, specA + (size_t)x * kPlane, lane, v);
+    slab_forward(R, specA + (size_t)x * kPlane, lane);
 }
 
 // ---------------------------------------------------------------- combine
@@ -151,9 +155,8 @@ __device__ __forceinline__ void combine_slab(const PropsArgs<float> &a, int s, i
     const int sn = s + 1;
     float *qn = a.hist + hoff(g, slot, sn, fld) + slab_r;
     const int z = 2 * lane;
-    float2 v[64];
     if (mode == 0) {
-        slab_inverse(specA + (size_t)x * kPlane, R, lane, v);
+        slab_inverse(specA + (size_t)x * kPlane, R, lane);
         const float *E = eptr(a, slot, esel(g, fld, s)) + slab_r;
         const float *P = a.pbuf + ((size_t)slot * 2 + fld) * kM + slab_r;
 #pragma unroll 4
@@ -188,7 +191,7 @@ __device__ __forceinline__ void combine_slab(const PropsArgs<float> &a, int s, i
         const float2 e = *reinterpret_cast<const float2 *>(En + y * 64 + z);
         *cp = make_float2(c.x * e.x, c.y * e.y);
     }
-    slab_forward(R, specA + (size_t)x * kPlane, lane, v);
+    slab_forward(R, specA + (size_t)x * kPlane, lane);
     // full step input E2' q' (q' re-read from the propagator store: this lane wrote it above)
 #pragma unroll 4
     for (int y = 0; y < 64; y++) {
@@ -196,7 +199,7 @@ __device__ __forceinline__ void combine_slab(const PropsArgs<float> &a, int s, i
         const float2 e = *reinterpret_cast<const float2 *>(En + y * 64 + z);
         *reinterpret_cast<float2 *>(R + y * kRowPitch + z) = make_float2(q.x * (e.x * e.x), q.y * (e.y * e.y));
     }
-    slab_forward(R, specB + (size_t)x * kPlane, lane, v);
+    slab_forward(R, specB + (size_t)x * kPlane, lane);
 }
 
 __global__ void __launch_bounds__(kPencilThreads) k_pencil_r(PropsArgs<float> a, int both)
@@ -305,9 +308,9 @@ bool reg64_applicable(int m0, int m1, int m2) { return m0 == 64 && m1 == 64 && m
 
 int reg64_set_smem()
 {
-    cudaError_t e1 = cudaFuncSetAttribute(k_mid_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
-    cudaError_t e2 = cudaFuncSetAttribute(k_combine_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
-    cudaError_t e3 = cudaFuncSetAttribute(k_step_r, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabSmem);
+    cudaError_t e1 = raise_dyn_smem(k_mid_r, kSlabSmem);
+    cudaError_t e2 = raise_dyn_smem(k_combine_r, kSlabSmem);
+    cudaError_t e3 = raise_dyn_smem(k_step_r, kSlabSmem);
     return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess) ? 0 : 1;
 }
 

@@ -663,9 +663,11 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
     const int rt_slab_threads = L.slab_threads, rt_pencil_threads = L.pencil_threads;
     L.fixed = fixed_shape_id(g.m0, g.m1, g.m2);
     if (L.fixed) L.slab_threads = L.pencil_threads = fixed_shape_threads(L.fixed);
-    // 64^3 FP32: register-resident step kernels (reg64.cu) unless SCFT_NO_REG=1
-    L.reg = (T == 4 && reg64_applicable(g.m0, g.m1, g.m2)) ? 1 : 0;
-    if (const char *ev = getenv("SCFT_NO_REG")) L.reg = ev[0] == '1' ? 0 : L.reg;
+    // 64^3 FP32: the register-resident step kernels (reg64.cu) with SCFT_REG64=1;
+    // the shared-memory kernels otherwise (measured faster on a B200)
+    L.reg = 0;
+    if (const char *ev = getenv("SCFT_REG64"))
+        L.reg = (ev[0] == '1' && T == 4 && reg64_applicable(g.m0, g.m1, g.m2)) ? 1 : 0;
     L.pf = 0;
     if (L.fixed) {
         pf_smem_bytes(L.fixed, T == 4, L.mid_pf_smem, L.combine_pf_smem);

@@ -458,12 +458,12 @@ int launch_stress_chunk(const StressArgs<T> &a, const StressPairs &P, int slab_t
 template <typename T>
 int set_stress_smem(int slab_smem, int pencil_smem)
 {
-    cudaError_t e1 = cudaFuncSetAttribute(k_stress_slab_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem);
-    cudaError_t e2 = cudaFuncSetAttribute(k_stress_slab_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem);
-    cudaError_t e3 = cudaFuncSetAttribute(k_stress_pencil1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
-    cudaError_t e4 = cudaFuncSetAttribute(k_stress_pencil2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
-    cudaError_t e5 = cudaFuncSetAttribute(k_jn_slab<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem);
-    cudaError_t e6 = cudaFuncSetAttribute(k_jn_pencil<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pencil_smem);
+    cudaError_t e1 = raise_dyn_smem(k_stress_slab_fwd<T>, slab_smem);
+    cudaError_t e2 = raise_dyn_smem(k_stress_slab_mid<T>, slab_smem);
+    cudaError_t e3 = raise_dyn_smem(k_stress_pencil1<T>, pencil_smem);
+    cudaError_t e4 = raise_dyn_smem(k_stress_pencil2<T>, pencil_smem);
+    cudaError_t e5 = raise_dyn_smem(k_jn_slab<T>, slab_smem);
+    cudaError_t e6 = raise_dyn_smem(k_jn_pencil<T>, pencil_smem);
     return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess &&
             e5 == cudaSuccess && e6 == cudaSuccess) ? 0 : -1;
 }

@@ -30,7 +30,7 @@ def test_profiled_traffic_reads_the_committed_summary():
 def test_defaults(monkeypatch, argv, steps, warmup):
     monkeypatch.setattr(sys, "argv", ["bench.py", *argv])
     a = bench.parse()
-    assert (a.gpus, a.steps, a.warmup, a.impl, a.precision, a.workload) == (1, steps, warmup, "ours", "fp32",
+    assert (a.gpus, a.steps, a.warmup, a.impl, a.precision, a.workload) == (1, steps, warmup, "ours", "fp64",
                                                                             "string")
     assert a.warmup >= 3
 

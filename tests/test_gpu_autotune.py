@@ -41,6 +41,8 @@ def test_persistent_step_launch_matches_four_launches(built_lib, monkeypatch):
     c = dict(STRING_64, N=40, strn=4)
     wm, wp = fields(c)
 
+    monkeypatch.setenv("SCFT_REG64", "1")
+
     def run(no_persist):
         if no_persist:
             monkeypatch.setenv("SCFT_NO_PERSIST", "1")

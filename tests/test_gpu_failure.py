@@ -122,3 +122,28 @@ def test_string_resume_continues_the_run(built_lib, prec):
     assert tail[3]["did_freee"] == 1  # k = 50
     for ii in range(c["strn"]):
         assert np.array_equal(a.get_fields(ii), r.get_fields(ii))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_smaller_context_keeps_larger_contexts_launchable(built_lib, prec):
+    """The runtime-shaped kernels serve every context: creating a context of
+    a small grid (and running its adjoint) after one of a large grid must not
+    lower the shared-memory limit the large one launches with."""
+    big, small = (30, 28, 24), (6, 5, 9)
+    wm, wp = _fields(big)
+    a = S.Context(big, (4.0, 4.0, 3.5), 20, chi=12.0, f=0.45, phidb=0.8, ens=2, strn=1, dostring=0, precision=prec)
+    a.set_fields(0, wm, wp)
+    a.props(0)
+    ref = a.get_conc(0)
+    _, sref = a.stress(0)
+    b = S.Context(small, (2.0, 2.0, 3.0), 20, chi=12.0, f=0.45, phidb=0.8, ens=2, strn=1, dostring=0,
+                  precision=prec)
+    bw, bp = _fields(small)
+    b.set_fields(0, bw, bp)
+    b.props(0)
+    b.stress(0)
+    a.props(0)
+    got = a.get_conc(0)
+    assert np.array_equal(got[0], ref[0]) and got[1] == ref[1]
+    _, s2 = a.stress(0)
+    assert np.array_equal(s2, sref)

@@ -129,3 +129,34 @@ def test_do_step_fixed_shapes(built_lib, m, prec, tol):
         ref = od.do_step(qin, s, 8, 8)
         got = ctx.do_step(0, qin, s)
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (m, s)
+
+
+@pytest.mark.parametrize("persist", ["0", "1"])
+def test_register_kernels_64cubed_fp32(built_lib, monkeypatch, persist):
+    """The register-resident 64^3 FP32 step kernels (SCFT_REG64=1), with four
+    launches per contour step or one persistent launch: one step against the
+    FP64 oracle at the FP32 step tolerance, and a props of the same fields
+    against the oracle's lnQ and densities."""
+    monkeypatch.setenv("SCFT_REG64", "1")
+    monkeypatch.setenv("SCFT_NO_PERSIST", "0" if persist == "1" else "1")
+    m = (64, 64, 64)
+    M = int(np.prod(m))
+    D = (4.0, 4.0, 4.0)
+    Ns, f = 16, 0.5
+    wm, wp = fields(m, 11, 1.0)
+    ctx = S.Context(m, D, Ns, chi=10, f=f, phidb=0.8, ens=2, strn=1, dostring=0, precision="fp32")
+    ctx.set_fields(0, wm, wp)
+    od = O.Density(m, D, Ns)
+    od.prepare(1.0 / Ns, np.concatenate([wm, wp]))
+    qin = 1.0 + 0.3 * np.random.default_rng(4).normal(size=2 * M)
+    for s in [0, 7, 8, Ns - 1]:
+        ref = od.do_step(qin, s, 8, 8)
+        got = ctx.do_step(0, qin, s)
+        assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max(), s
+    ctx.props(0)
+    conc, lnQ, phis = ctx.get_conc(0)
+    w0 = np.zeros(6 * M)
+    w0[:M], w0[M:2 * M] = wm, wp
+    lnQ0, phis0 = O.Density(m, D, Ns).props(w0, Ns, 0.1, 0.8, f, 2)
+    assert abs(lnQ - lnQ0) <= 1e-5 * abs(lnQ0)
+    assert np.abs(conc - w0[2 * M:]).max() <= 1e-5

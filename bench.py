@@ -54,6 +54,10 @@ def parse():
                     help="tolerance: errtot at which the FP32 iterations hand the string to FP64")
     ap.add_argument("--max-iters", type=int, default=4000,
                     help="tolerance: string iteration cap (the reference's nsterp, scft.cu:1102)")
+    ap.add_argument("--case", default="string64", choices=["string64", "plain32"],
+                    help="tolerance: the 16-replica 64^3 string, or the 32^3 single-replica workload")
+    ap.add_argument("--compare", action="store_true",
+                    help="tolerance: run FP32 -> FP64 and FP64 only, and compare their final F")
     ap.add_argument("--time-limit", type=float, default=0.0,
                     help="tolerance: stop (reached = false) after this many wall seconds (0: none)")
     ap.add_argument("--tol", type=float, default=1e-5, help="uneven24: RMS residual target")
@@ -296,30 +300,27 @@ def run_uneven(a):
     return 0
 
 
-def run_tolerance(a):
-    """Time to the metric's error clause on the 16-replica 64^3 string: the
-    reference's solve_field iterations (scft.cu:592-806; its loop never stops
-    on the error, scft.cu:563) run until errtot = sqrt(mean errs3^2)
-    (scft.cu:764-765) <= --tol, or --max-iters.
-      --precision fp32: FP32 batched iterations until errtot <= --switch (or
-        no 1 % progress over 200 iterations), then the fields go device to
-        device to an FP64 batched context that continues the same run (same k)
-        to --tol; F per replica from a final FP64 FreeE;
-      --precision fp64: FP64 batched from the start.
+def tolerance_run(a, cfg, precision):
+    """One run of the reference's solve_field iterations (scft.cu:592-806;
+    its loop never stops on the error, scft.cu:563) until errtot =
+    sqrt(mean errs3^2) (scft.cu:764-765) <= a.tol, a.max_iters or
+    a.time_limit, after the W+ prelude (scft.cu:1105).
+      precision fp32: FP32 batched iterations until errtot <= a.switch (or no
+        1 % progress over 200 iterations), then the fields go device to device
+        to an FP64 batched context that continues the same run (same k) to
+        a.tol; F per replica from a final FP64 FreeE;
+      precision fp64: FP64 batched from the start.
     Device time per phase (CUDA events on each context's stream), the errtot
-    history, F per replica, and -- at the hand-over -- the FP32 errors
-    against FP64 at identical fields."""
+    history, F per replica, and -- at the hand-over -- the FP32 errors against
+    FP64 at identical fields."""
     import numpy as np
-    import torch
 
     import scft_string_b200 as S
-    from scft_string_b200.configs import STRING_64, fields
-    torch.cuda.set_device(0)
-    cfg = dict(STRING_64)
+    from scft_string_b200.configs import fields
     strn, M = cfg["strn"], int(np.prod(cfg["m"]))
     wm, wp = fields(cfg)
     t_wall = time.time()
-    first = S.StringSolver(cfg, precision=a.precision, batched=True)
+    first = S.StringSolver(cfg, precision=precision, batched=True)
     for ii in range(strn):
         first.set_fields(ii, wm[ii], wp[ii])
     first.autotune()
@@ -328,6 +329,8 @@ def run_tolerance(a):
     first.timer_mark(1)
     prelude_ms = first.timer_elapsed_ms(0, 1)
     hist = []
+    out = {"workload": "tolerance: " + cfg["name"], "tol": a.tol, "mode": precision, "max_iters": a.max_iters,
+           "prelude_s": prelude_ms / 1e3}
 
     def phase(ctx, k0, stop_tol, stall):
         ctx.string_resume(k0, a.max_iters, 1e-3)
@@ -347,13 +350,11 @@ def run_tolerance(a):
                 break
         ctx.timer_mark(3)
         st = ctx.stats()
-        return k, dict(iters=k - k0, seconds=ctx.timer_elapsed_ms(2, 3) / 1e3, errtot_end=hist[-1][1],
+        return k, dict(iters=k - k0, seconds=ctx.timer_elapsed_ms(2, 3) / 1e3, errtot_end=hist[-1][1] if hist else None,
                        props_per_replica_iter=st["props_calls"] / max(1, (k - k0) * strn),
                        contour_steps_per_s=st["contour_steps"] / max(1e-30, st["props_seconds"]))
 
-    out = {"workload": "tolerance: " + cfg["name"], "tol": a.tol, "mode": a.precision, "max_iters": a.max_iters,
-           "prelude_s": prelude_ms / 1e3}
-    if a.precision == "fp32":
+    if precision == "fp32":
         k, p32 = phase(first, 0, a.switch, True)
         out["phase_fp32"] = p32
         W = [np.ascontiguousarray(first.get_fields(ii)) for ii in range(strn)]
@@ -374,7 +375,7 @@ def run_tolerance(a):
             dd.append(float(np.sqrt(np.mean((d32 - d64) ** 2))))
         one64.close()
         one32.close()
-        out["fp32_errors_at_handover"] = {"F_per_chain": dF, "lnQ_rel": dq, "rhoA_maxabs": dr,
+        out["fp32_errors_at_handover"] = {"k": k, "F_per_chain": dF, "lnQ_rel": dq, "rhoA_maxabs": dr,
                                           "exchange_residual_rms_diff": dd}
         second = S.StringSolver(cfg, precision="fp64", batched=True)
         second.autotune()
@@ -389,14 +390,36 @@ def run_tolerance(a):
         out["phase_fp64"] = p64
         last = first
     fe = last.free_energy()
+    last.close()
     out["reached"] = bool(hist and hist[-1][1] <= a.tol)
     out["iterations"] = k
     out["time_to_tol_s"] = sum(out[p]["seconds"] for p in ("phase_fp32", "phase_fp64") if p in out)
     out["time_to_tol_with_prelude_s"] = out["time_to_tol_s"] + out["prelude_s"]
     out["iters_per_s"] = k / max(1e-30, out["time_to_tol_s"])
     out["F_per_replica_fp64"] = list(fe["FEs"])
-    out["errtot_history"] = hist[::10] + [hist[-1]]
+    out["errtot_history"] = hist[::10] + hist[-1:]
     out["wall_s"] = time.time() - t_wall
+    return out
+
+
+def run_tolerance(a):
+    """Time to the metric's error clause (tolerance_run) on the 16-replica 64^3
+    string, or on the 32^3 single-replica workload (--case plain32).  With
+    --compare, both the FP32 -> FP64 run and the FP64-only run, and the
+    difference of their final F per replica."""
+    import torch
+
+    from scft_string_b200.configs import PLAIN_32, STRING_64
+    torch.cuda.set_device(0)
+    cfg = dict(STRING_64 if a.case == "string64" else PLAIN_32)
+    if a.compare:
+        runs = {p: tolerance_run(a, cfg, p) for p in ("fp32", "fp64")}
+        F32, F64 = runs["fp32"]["F_per_replica_fp64"], runs["fp64"]["F_per_replica_fp64"]
+        out = {"workload": "tolerance: " + cfg["name"], "fp32_then_fp64": runs["fp32"], "fp64_only": runs["fp64"],
+               "F_diff_per_chain": [abs(x - y) for x, y in zip(F32, F64)],
+               "time_ratio_fp64_only_over_mixed": runs["fp64"]["time_to_tol_s"] / max(1e-30, runs["fp32"]["time_to_tol_s"])}
+    else:
+        out = tolerance_run(a, cfg, a.precision)
     print(json.dumps(out))
     return 0
 

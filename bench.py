@@ -627,7 +627,7 @@ def run_ours(a, cfg, rank, world, dev):
     ctx = S.StringSolver(cfg, precision=a.precision, batched=not a.plain, device=dev)
     for ii in range(strn):
         ctx.set_fields(ii, wm[ii], wp[ii])
-    groups, wide, tune_ms = ctx.autotune()     # slot groups and pencil tile width per props round
+    groups, wide, persist, tune_ms = ctx.autotune()  # slot groups, pencil tiles, launches per step
     ctx.solve_field0_all(5000, 1e-4)           # prelude, scft.cu:1105
     nsterp = 4000                              # scft.cu:1102
     M = ctx.M
@@ -675,7 +675,9 @@ def run_ours(a, cfg, rank, world, dev):
     out = dict(ms=ms_max, reps=reps, stats=st, clocks=clocks, e2e_ms=e2e_ms, ctx=ctx, M=M, W0=W0,
                e2e_same_iterations=same,
                schedule={"slot_groups": groups, "wide_pencil_tiles": bool(wide),
-                         "props_round_ms": dict(zip(["g1_tile1", "g2_tile1", "g1_tile2", "g2_tile2"], tune_ms))})
+                         "persistent_step_launch": bool(persist),
+                         "props_round_ms": {f"g{1 + (c & 1)}_tile{1 + ((c >> 1) & 1)}_{'persistent' if c >> 2 else 'four'}":
+                                            v for c, v in enumerate(tune_ms) if v > 0}})
     # ---- the other precision (batched) and plain FP64 on the same window
     if rank == 0 and world == 1 and not a.no_fp64:
         other = "fp64" if a.precision == "fp32" else "fp32"

@@ -276,16 +276,23 @@ scft_status scft_load_checkpoint(scft_ctx *ctx, const char *path);
  * its content. */
 scft_status scft_checkpoint_info(const char *path, int *version, int *strn, int *m, double *D);
 /* Picks the schedule of a props round by timing rounds of all replicas at
- * their current fields: 1 or 2 concurrent slot groups, times a second choice
- * -- x-pencil tiles of the default or twice the width (grids with tensor-map
- * pencils), or, on 64^3 FP32 contexts (register-resident step kernels), four
- * launches per contour step or one persistent launch per step.  The
- * densities are recomputed, the statistics left unchanged.  *groups_out,
- * *wide_out = the setting kept (wide_out: 1 = wide tiles, or the persistent
- * launch); times_ms[0..3] = best round time for (1 group, first choice),
- * (2, first), (1, second), (2, second), -1 where not available (any pointer
- * may be NULL).  Performance-only: results do not depend on the setting. */
+ * their current fields: 1 or 2 concurrent slot groups, and x-pencil tiles of
+ * the default or twice the width (grids with tensor-map pencils), each with
+ * four launches per contour step and, where the context has it, one
+ * persistent launch per step (see scft_autotune_ex).  The densities are
+ * recomputed, the statistics left unchanged.  *groups_out, *wide_out = the
+ * setting kept; times_ms[0..3] = best round time with four launches per step
+ * for (1 group, default tile), (2, default), (1, wide), (2, wide), -1 where
+ * not available (any pointer may be NULL).  Performance-only: results do not
+ * depend on the setting. */
 scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms);
+/* scft_autotune over a third axis as well: four launches per contour step, or
+ * one persistent launch per step (work items claimed in order, bounded
+ * waits), where the context has one (compile-time grid shapes).  times_ms[c]
+ * for c = (groups - 1) + 2 wide + 4 persist, -1 where not available;
+ * *persist_out = the launch form kept.  Performance-only: results do not
+ * depend on the setting. */
+scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int *persist_out, double *times_ms);
 
 #ifdef __cplusplus
 }

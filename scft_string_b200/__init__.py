@@ -81,7 +81,7 @@ EXPORTS = [
     "scft_anderson_solve", "scft_autotune", "scft_stress_ckpt", "scft_dF_df",
     "scft_save_checkpoint", "scft_load_checkpoint", "scft_set_box_replica", "scft_get_box_replica",
     "scft_gradients", "scft_props_ckpt", "scft_checkpoint_info", "scft_string_resume",
-    "scft_selftest_timeout", "scft_copy_fields",
+    "scft_selftest_timeout", "scft_copy_fields", "scft_autotune_ex",
 ]
 
 _lib = None
@@ -141,6 +141,7 @@ def lib():
     L.scft_relax_cell.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp]
     L.scft_timer_elapsed.argtypes = [vp, C.c_int, C.c_int, _dp]
     L.scft_autotune.argtypes = [vp, _ip, _ip, _dp]
+    L.scft_autotune_ex.argtypes = [vp, _ip, _ip, _ip, _dp]
     L.scft_stress_ckpt.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp]
     L.scft_dF_df.argtypes = [vp, C.c_int, _dp, _dp]
     L.scft_save_checkpoint.argtypes = [vp, C.c_char_p]
@@ -464,12 +465,13 @@ class Context:
         return v.value
 
     def autotune(self):
-        """(slot groups kept, wide pencil tiles kept, best props-round times in ms for
-        (1 group, default tile), (2, default), (1, wide), (2, wide); -1 where not available)."""
-        g, w = C.c_int(), C.c_int()
-        t = np.zeros(4)
-        self._ck(lib().scft_autotune(self.h, C.byref(g), C.byref(w), _p(t)))
-        return g.value, w.value, [float(v) for v in t]
+        """(slot groups kept, wide pencil tiles kept, persistent step launch kept,
+        best props-round times in ms indexed (groups - 1) + 2 wide + 4 persistent;
+        -1 where not available)."""
+        g, w, p = C.c_int(), C.c_int(), C.c_int()
+        t = np.zeros(8)
+        self._ck(lib().scft_autotune_ex(self.h, C.byref(g), C.byref(w), C.byref(p), _p(t)))
+        return g.value, w.value, p.value, [float(v) for v in t]
 
     def save_checkpoint(self, path):
         """Binary FP64 checkpoint of box and fields of every replica."""

@@ -62,8 +62,10 @@ struct PropsLaunch {
     int pencil_tma_smem_wide;
     const CUtensorMap *tmap_wide;  // the same spectra with the wide tile box
     int reg;         // 64^3 FP32: register-resident step kernels (reg64.cu) instead of the shared-memory ones
-    int persist;     // with reg: one persistent launch per contour step instead of four
-    int step_grid;   // CTAs of that launch
+    int persist;     // one persistent launch per contour step instead of four (register kernels, or the
+                     // shared-memory kernels of the compile-time shapes)
+    int step_grid;   // CTAs of the register kernels' persistent launch
+    int step_grid_pf, step_pf_smem;  // CTAs and dynamic shared memory of the shared-memory kernels' one
 };
 
 // register-resident 64^3 FP32 step kernels (reg64.cu)
@@ -87,6 +89,9 @@ template <typename T>
 int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaStream_t st);
 template <typename T>
 int set_props_smem(const PropsLaunch &L);
+// CTAs of the persistent step kernel of the compile-time shapes (0: none)
+template <typename T>
+int props_step_grid(const PropsLaunch &L);
 // chain segment of slot 0 (a.g.Ns steps; a.g.n1, n2 relative to the segment
 // start), E tables of slot 0 from its replica, Q2/QC/lnQ of slot 0 from the
 // store slices a.g.Ns (q) and a.g.Nh (q^dagger)

@@ -359,11 +359,12 @@ struct SlabSmem {
     static constexpr int combine_bytes() { return BARS + (SLAB_C + M1 + M2) * 2 * (int)sizeof(T) + 2 * REAL_BYTES; }
 };
 
+// slab x of (slot, fld); the body of k_mid_pf and of the persistent step kernel
 template <typename T, int MT, int FM0, int FM1, int FM2>
-__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_mid_pf(PropsArgs<T> a, int s)
+__device__ __forceinline__ void mid_pf_body(const PropsArgs<T> &a, int s, int x, int fld, int slot,
+                                            unsigned char *smem_raw)
 {
     using L = SlabSmem<T, FM1, FM2>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     const Geo &g = a.g;
     constexpr int m1 = FM1, m2 = FM2, mk2 = L::MK2, M = FM0 * FM1 * FM2, Mk = FM0 * FM1 * L::MK2;
     constexpr int npz = ((m1 + 1) / 2) * m2;
@@ -373,7 +374,6 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     cplx<T> *twy = bufB + L::SLAB_C;
     cplx<T> *twz = twy + m1;
     T *E4s = reinterpret_cast<T *>(twz + m2);
-    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
     const T *E4g = etab_ptr(a, slot, etab_sel(g, fld, s)) + slab_r;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
@@ -430,10 +430,10 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
 
 // combine with prefetch: mode 0 (Richardson), 1 (q = 1), 2 (q from the store)
 template <typename T, int MT, int FM0, int FM1, int FM2>
-__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_combine_pf(PropsArgs<T> a, int s, int mode)
+__device__ __forceinline__ void combine_pf_body(const PropsArgs<T> &a, int s, int mode, int x, int fld, int slot,
+                                                unsigned char *smem_raw)
 {
     using L = SlabSmem<T, FM1, FM2>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     const Geo &g = a.g;
     constexpr int m1 = FM1, m2 = FM2, mk2 = L::MK2, M = FM0 * FM1 * FM2, Mk = FM0 * FM1 * L::MK2;
     constexpr int npz = ((m1 + 1) / 2) * m2;
@@ -443,7 +443,6 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
     cplx<T> *twz = twy + m1;
     T *Q = reinterpret_cast<T *>(twz + m2);  // P, then q'
     T *E = Q + L::REAL;                        // E4 of step s (or of step s+1)
-    const int x = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const size_t slab_r = (size_t)x * m1 * m2, slab_k = (size_t)x * m1 * mk2;
     cplx<T> *specA = a.spec + ((size_t)slot * 2 + fld) * 2 * Mk;
     cplx<T> *specB = specA + Mk;
@@ -543,10 +542,9 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) 
 // Both spectra of a both-pass are requested at kernel start, so the second
 // one lands while the first is transformed; results leave through tile stores.
 template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
-__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
-    k_pencil_tma(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int both)
+__device__ __forceinline__ void pencil_tma_body(const CUtensorMap &tmap, const PropsArgs<T> &a, int both, int tile,
+                                                int fld, int slot, unsigned char *smem_raw)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int m0 = FM0, m1 = FM1, mk2 = FM2 / 2 + 1;
     constexpr int BOX = TC * m0;                      // complex elements per tile
     constexpr uint32_t BOX_BYTES = BOX * 2 * sizeof(T);
@@ -556,7 +554,6 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     cplx<T> *twx = bufB + BOX;
     T *colf = reinterpret_cast<T *>(twx + m0);
     T *gx = colf + TC;
-    const int tile = blockIdx.x, fld = blockIdx.y, slot = blockIdx.z;
     const int ncol = m1 * mk2, c0 = tile * TC;
     const int x = 2 * c0;
     const int y0 = (((a.slot0 + slot) * 2 + fld) * 2) * m0;
@@ -601,6 +598,157 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
         if (threadIdx.x == 0) tma_store_2d(&tmap, x, y0 + pass * m0, buf);
     }
     if (threadIdx.x == 0) tma_store_wait_read();
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
+    k_pencil_tma(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int both)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    pencil_tma_body<T, MT, FM0, FM1, FM2, TC>(tmap, a, both, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_mid_pf(PropsArgs<T> a, int s)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    mid_pf_body<T, MT, FM0, FM1, FM2>(a, s, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_combine_pf(PropsArgs<T> a, int s, int mode)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    combine_pf_body<T, MT, FM0, FM1, FM2>(a, s, mode, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// ---------------------------------------------------------------- one launch per contour step
+// The persistent form of the four launches above for the compile-time
+// shapes: CTAs claim work items from a counter in a fixed order -- every
+// pencil(both) tile, then every mid slab, every pencil(A) tile, every combine
+// slab, each phase ordered by (slot, field) -- and an item waits only for the
+// items of the previous phase of its own (slot, field).  Items are claimed in
+// order by running CTAs, so whatever an item waits for is held by a CTA that
+// is running or done: no residency assumption is needed.  Completion
+// counters are cumulative over the steps of a props round (n_p (s+1) items of
+// phase p are done after step s) and zeroed with the claim counters when the
+// round starts.  Every wait is bounded (2^22 polls of ~32 ns) and records
+// error 3 when it gives up, which ends the kernel.
+//
+// The items move data between CTAs of one launch through both proxies: tile
+// stores (async proxy) feed the slab kernels' bulk loads, and the slab
+// kernels' generic stores feed the next pencil's tile loads.  A producer waits
+// for its bulk stores to complete, fences the async proxy against the generic
+// one and releases its counter; a consumer acquires the counter and fences the
+// generic proxy against the async one before it issues bulk loads.  Shared
+// memory is reused across items, so every item starts with an async-proxy
+// fence over the previous item's generic shared accesses, and the mbarriers
+// of an item are invalidated before the next one initialises them.
+constexpr uint32_t kStepSpinPF = 1u << 22;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_wait_all()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// The three roles out of line: each is then register-allocated as in its own
+// kernel; inlined together they spilled kilobytes per thread.
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__device__ __noinline__ void pencil_tma_call(const CUtensorMap *tmap, const PropsArgs<T> *a, int both, int tile,
+                                             int fld, int slot, unsigned char *smem_raw)
+{
+    pencil_tma_body<T, MT, FM0, FM1, FM2, TC>(*tmap, *a, both, tile, fld, slot, smem_raw);
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__device__ __noinline__ void mid_pf_call(const PropsArgs<T> *a, int s, int x, int fld, int slot, unsigned char *smem_raw)
+{
+    mid_pf_body<T, MT, FM0, FM1, FM2>(*a, s, x, fld, slot, smem_raw);
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2>
+__device__ __noinline__ void combine_pf_call(const PropsArgs<T> *a, int s, int x, int fld, int slot,
+                                             unsigned char *smem_raw)
+{
+    combine_pf_body<T, MT, FM0, FM1, FM2>(*a, s, 0, x, fld, slot, smem_raw);
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
+    k_step_pf(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int s, int nslots)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ int item_sh, ok_sh;
+    constexpr int ntiles = (FM1 * (FM2 / 2 + 1) + TC - 1) / TC;
+    const int G = 2 * nslots;  // (slot, field) groups
+    const int per[4] = {ntiles, FM0, ntiles, FM0};
+    const int total = G * (2 * ntiles + 2 * FM0);
+    int *claim = a.sync + s;      // this step's claim counter
+    int *done = a.sync + a.g.Ns;  // [phase][group] completion counters
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    for (;;) {
+        fence_proxy_async_smem();
+        if (threadIdx.x == 0) item_sh = atomicAdd(claim, 1);
+        __syncthreads();
+        int it = item_sh;
+        if (it >= total) break;
+        int phase = 0;
+        while (it >= G * per[phase]) {
+            it -= G * per[phase];
+            phase++;
+        }
+        const int group = it / per[phase], unit = it - group * per[phase];
+        const int slot = group >> 1, fld = group & 1;
+        if (phase > 0) {
+            if (threadIdx.x == 0) {
+                const int need = per[phase - 1] * (s + 1);
+                const int *cnt = done + (phase - 1) * G + group;
+                uint32_t i = 0;
+                while (ld_acquire_gpu(cnt) < need && i < kStepSpinPF) {
+                    __nanosleep(32);
+                    i++;
+                }
+                ok_sh = i < kStepSpinPF;
+                if (!ok_sh) *a.err = 3;
+                fence_proxy_async_global();
+            }
+            __syncthreads();
+            if (!ok_sh) return;
+        }
+        int nbar;
+        if (phase == 0 || phase == 2) {
+            pencil_tma_call<T, MT, FM0, FM1, FM2, TC>(&tmap, &a, phase == 0, unit, fld, slot, smem_raw);
+            nbar = 2;
+            if (threadIdx.x == 0) {
+                bulk_wait_all();  // the tile stores have reached global memory
+                fence_proxy_async_global();
+            }
+        } else if (phase == 1) {
+            mid_pf_call<T, MT, FM0, FM1, FM2>(&a, s, unit, fld, slot, smem_raw);
+            nbar = 3;
+        } else {
+            combine_pf_call<T, MT, FM0, FM1, FM2>(&a, s, unit, fld, slot, smem_raw);
+            nbar = 3;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < nbar; i++) mbar_inval(&bars[i]);
+            __threadfence();
+            atomicAdd(done + phase * G + group, 1);
+        }
+    }
 }
 
 // ---------------------------------------------------------------- bounded-wait self-test
@@ -904,6 +1052,22 @@ int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cud
             n += g.Ns;
         }
     }
+    if constexpr (F1 != 0) {
+        if (n == 6 && !L.reg && L.persist && L.pf && L.tma_pencil && a.sync) {
+            // one persistent launch per contour step on the shared-memory kernels
+            constexpr int TC = kTile<T>::value;
+            cudaMemsetAsync(a.sync, 0, sizeof(int) * reg64_sync_ints(g.Ns, nslots), st);
+            launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
+            for (int s = 0; s < g.Ns; s++) {
+                if (L.ptile_wide)
+                    k_step_pf<T, MT, F0, F1, F2, 2 * TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(*L.tmap_wide, a, s,
+                                                                                                    nslots);
+                else
+                    k_step_pf<T, MT, F0, F1, F2, TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(*L.tmap, a, s, nslots);
+            }
+            n += g.Ns;
+        }
+    }
     if (n == 6) {
         launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
         for (int s = 0; s < g.Ns; s++) {
@@ -975,6 +1139,14 @@ int set_smem_mt(const PropsLaunch &L)
     }
     int e6 = 0;
     if constexpr (kReg64<T, F0, F1, F2>) e6 = reg64_set_smem();
+    if constexpr (F1 != 0) {
+        if (L.pf && L.tma_pencil && L.step_pf_smem > 0) {
+            constexpr int TC = kTile<T>::value;
+            if (raise_dyn_smem(k_step_pf<T, MT, F0, F1, F2, TC>, L.step_pf_smem) != cudaSuccess) e6 = 1;
+            if (L.tmap_wide && raise_dyn_smem(k_step_pf<T, MT, F0, F1, F2, 2 * TC>, L.step_pf_smem) != cudaSuccess)
+                e6 = 1;
+        }
+    }
     return (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess && e5 == cudaSuccess &&
             e6 == 0)
                ? 0
@@ -1004,12 +1176,28 @@ void pf_smem_bytes(int id, int fp32, int &mid, int &comb)
         pf_smem<double>(id, mid, comb);
 }
 
-// op 0: props, 1: single step, 2: shared-memory attributes, 3: chain segment
+// op 0: props, 1: single step, 2: shared-memory attributes, 3: chain segment, 4: CTAs of the
+// persistent step kernel
 template <typename T, int MT, int F0, int F1, int F2>
 int run_op(int op, const PropsArgs<T> *a, const PropsLaunch &L, int n, cudaStream_t st)
 {
     if (op == 0) return launch_props_mt<T, MT, F0, F1, F2>(*a, L, n, st);
     if (op == 1) return launch_single_step_mt<T, MT, F0, F1, F2>(*a, L, n, st);
+    if (op == 4) {
+        // CTAs of the persistent step kernel: the occupancy of its larger (wide) form times the SMs
+        if constexpr (F1 != 0) {
+            constexpr int TC = kTile<T>::value;
+            int dev = 0, sms = 148, per_sm = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaError_t e = L.tmap_wide
+                                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_pf<T, MT, F0, F1, F2, 2 * TC>,
+                                                                                MT, L.step_pf_smem)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_pf<T, MT, F0, F1, F2, TC>, MT,
+                                                                                L.step_pf_smem);
+            return (e == cudaSuccess && per_sm > 0) ? sms * per_sm : 0;
+        }
+        return 0;
+    }
     if (op == 3) return launch_chain_mt<T, MT, F0, F1, F2>(*a, L, n, st);
     return set_smem_mt<T, MT, F0, F1, F2>(L);
 }
@@ -1050,6 +1238,14 @@ int launch_single_step(const PropsArgs<T> &a, const PropsLaunch &L, int s, cudaS
 {
     return dispatch<T>(1, &a, L, s, st);
 }
+
+template <typename T>
+int props_step_grid(const PropsLaunch &L)
+{
+    return dispatch<T>(4, nullptr, L, 0, nullptr);
+}
+template int props_step_grid<float>(const PropsLaunch &);
+template int props_step_grid<double>(const PropsLaunch &);
 
 template <typename T>
 int set_props_smem(const PropsLaunch &L)

@@ -81,6 +81,7 @@ struct scft_ctx {
     int *rep_dev = nullptr, *err = nullptr;
     int *sync = nullptr;     // counters of the persistent step kernel, one block per slot group
     int sync_stride = 0;
+    bool persist_ok = false; // a persistent step launch exists for this context
     std::vector<double> Dr;  // box of every replica (3 per replica); p.D is the last common box
     int kf_n = 0;            // diffusion factors per replica (m0 + m1 + mk2)
     void *jtab = nullptr;  // junction-step E table per slot (continuous A fraction)
@@ -297,7 +298,7 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
                 if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
             }
             CK(cudaGraphLaunch(ctx->graphs[key], ctx->st));
-            launches += ((ctx->L.reg && ctx->L.persist ? 1 : 4) * ctx->g.Ns + 6) * ng;
+            launches += ((ctx->L.persist ? 1 : 4) * ctx->g.Ns + 6) * ng;
         } else {
             launches += launch();
         }
@@ -738,7 +739,7 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaMalloc(&ctx->hist, ctx->nostore ? T * 2 * M : T * 2 * M * (size_t)(g.Ns + 1) * S));
         CKC(cudaMalloc(&ctx->spec, T * 2 * 4 * (size_t)g.Mk * S));
         CKC(cudaMalloc(&ctx->pbuf, T * 2 * M * S));
-        if (L.reg) {
+        if (L.reg || L.fixed) {  // counters of the persistent step launch
             ctx->sync_stride = reg64_sync_ints(g.Ns, (int)S);
             CKC(cudaMalloc(&ctx->sync, sizeof(int) * 2 * (size_t)ctx->sync_stride));
         }
@@ -797,6 +798,14 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
                 }
             }
         }
+        // the persistent step kernel of the compile-time shapes runs all three
+        // roles in one CTA shape: the largest of their shared-memory layouts
+        L.step_pf_smem = 0;
+        if (L.fixed && L.pf && L.tma_pencil) {
+            int sm = std::max(L.mid_pf_smem, std::max(L.combine_pf_smem, L.pencil_tma_smem));
+            if (L.tmap_wide) sm = std::max(sm, L.pencil_tma_smem_wide);
+            if (sm <= (int)prop.sharedMemPerBlockOptin) L.step_pf_smem = sm;
+        }
         if ((T == 4 ? set_props_smem<float>(L) : set_props_smem<double>(L)) != 0) {
             ctx->lasterr = "cudaFuncSetAttribute(max dynamic shared memory) failed";
             rc = SCFT_CUDA_ERROR;
@@ -804,12 +813,20 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         }
         // register kernels: one persistent launch per contour step unless SCFT_NO_PERSIST=1
         // (scft_autotune compares it with four launches per step)
+        // one persistent launch per contour step: the register kernels start with
+        // it, the shared-memory kernels with four launches (scft_autotune compares
+        // both); SCFT_PERSIST=0|1 sets the start, SCFT_NO_PERSIST=1 rules it out
         L.persist = 0;
+        L.step_grid_pf = L.step_pf_smem > 0 ? (T == 4 ? props_step_grid<float>(L) : props_step_grid<double>(L)) : 0;
         if (L.reg) {
             L.step_grid = reg64_step_grid();
             L.persist = 1;
-            if (const char *ev = getenv("SCFT_NO_PERSIST")) L.persist = ev[0] == '1' ? 0 : 1;
         }
+        ctx->persist_ok = (L.reg || L.step_grid_pf > 0) && ctx->sync;
+        if (const char *ev = getenv("SCFT_PERSIST")) L.persist = ev[0] == '1' ? 1 : 0;
+        if (const char *ev = getenv("SCFT_NO_PERSIST"))
+            if (ev[0] == '1') ctx->persist_ok = false;
+        if (!ctx->persist_ok) L.persist = 0;
         ctx->doiis.assign(ctx->strn, 1);  // one process owns every replica (scft.cu:952-975)
         ctx->graphs.assign((size_t)(R + 1) * (S + 1) + 1, nullptr);
         if (const char *ev = getenv("SCFT_NO_GRAPHS")) ctx->use_graphs = ev[0] != '1';
@@ -2210,14 +2227,15 @@ scft_status scft_reset_stats(scft_ctx *ctx)
 // three timed rounds counts.  The rounds recompute every replica's densities
 // at its current fields, so the state a caller sees afterwards is unchanged;
 // the statistics are restored.
-scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms)
+scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int *persist_out, double *times_ms)
 {
     if (!ctx) return SCFT_BAD_INPUT;
+    if (times_ms)
+        for (int c = 0; c < 8; c++) times_ms[c] = -1;
     if (ctx->nostore) {  // props run one replica at a time from checkpoints: nothing to schedule
         if (groups_out) *groups_out = 1;
         if (wide_out) *wide_out = ctx->L.ptile_wide;
-        if (times_ms)
-            for (int c = 0; c < 4; c++) times_ms[c] = -1;
+        if (persist_out) *persist_out = 0;
         return SCFT_OK;
     }
     const scft_stats keep = ctx->stats;
@@ -2231,21 +2249,20 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
             }
     };
     double best = 0;
-    int best_g = 1, best_w = 0;
-    // second axis: x-pencil tile width, or -- with the register kernels, which
-    // have no pencil tiles -- one persistent launch per step against four
-    const bool reg = ctx->L.reg != 0;
-    const int nw = reg ? 2 : (ctx->L.tmap_wide ? 2 : 1);
-    for (int c = 0; c < 4; c++) {
-        const int ng = 1 + (c & 1), wide = c >> 1;
-        if (times_ms) times_ms[c] = -1;
-        if (wide >= nw) continue;
+    int best_g = 1, best_w = 0, best_p = 0;
+    bool first = true;
+    // axes: slot groups (1, 2) x x-pencil tile width (default, wide; tensor-map
+    // pencils of the shared-memory kernels only) x launches per contour step
+    // (four, or one persistent launch)
+    const int nw = (!ctx->L.reg && ctx->L.tmap_wide) ? 2 : 1;
+    const int np = ctx->persist_ok ? 2 : 1;
+    for (int c = 0; c < 8; c++) {
+        const int ng = 1 + (c & 1), wide = (c >> 1) & 1, persist = c >> 2;
+        if (wide >= nw || persist >= np) continue;
         drop_graphs();
         ctx->ngroups = ng;
-        if (reg)
-            ctx->L.persist = wide;
-        else
-            ctx->L.ptile_wide = wide;
+        ctx->L.ptile_wide = wide;
+        ctx->L.persist = persist;
         scft_status s = props_list(ctx, all);
         if (s != SCFT_OK) return s;
         double t = 1e300;
@@ -2256,22 +2273,32 @@ scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double 
             t = std::min(t, (ctx->stats.props_seconds - before) * 1e3);
         }
         if (times_ms) times_ms[c] = t;
-        if (c == 0 || t < best) {
+        if (first || t < best) {
+            first = false;
             best = t;
             best_g = ng;
             best_w = wide;
+            best_p = persist;
         }
     }
     drop_graphs();
     ctx->ngroups = best_g;
-    if (reg)
-        ctx->L.persist = best_w;
-    else
-        ctx->L.ptile_wide = best_w;
+    ctx->L.ptile_wide = best_w;
+    ctx->L.persist = best_p;
     ctx->stats = keep;
     if (groups_out) *groups_out = best_g;
     if (wide_out) *wide_out = best_w;
+    if (persist_out) *persist_out = best_p;
     return SCFT_OK;
+}
+
+scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms)
+{
+    double t8[8];
+    scft_status s = scft_autotune_ex(ctx, groups_out, wide_out, nullptr, t8);
+    if (times_ms)
+        for (int c = 0; c < 4; c++) times_ms[c] = t8[c];
+    return s;
 }
 
 // ---- binary FP64 checkpoint (no reference counterpart: the reference keeps

@@ -22,9 +22,9 @@ def test_autotune_schedules_give_identical_densities(built_lib, precision):
     for ii in range(c["strn"]):
         ctx.props(ii)
         ref.append(ctx.get_conc(ii))
-    groups, wide, t = ctx.autotune()
-    assert groups in (1, 2) and wide in (0, 1) and len(t) == 4
-    assert all(v > 0 for v in t), t          # 32^3 has tensor-map pencils: all four schedules ran
+    groups, wide, persist, t = ctx.autotune()
+    assert groups in (1, 2) and wide in (0, 1) and persist in (0, 1) and len(t) == 8
+    assert all(v > 0 for v in t), t          # 32^3: tensor-map pencils and the persistent launch, all eight ran
     for ii in range(c["strn"]):
         conc, lnq, phis = ctx.get_conc(ii)
         np.testing.assert_array_equal(conc, ref[ii][0])
@@ -65,9 +65,36 @@ def test_persistent_step_launch_matches_four_launches(built_lib, monkeypatch):
     for ii in range(c["strn"]):  # densities at the fields after the W+ update
         ctx.props(ii)
         ref.append(ctx.get_conc(ii)[0])
-    groups, persist, t = ctx.autotune()
-    assert groups in (1, 2) and persist in (0, 1) and all(v > 0 for v in t), t
+    groups, wide, persist, t = ctx.autotune()
+    assert groups in (1, 2) and wide == 0 and persist in (0, 1)
+    assert all(t[c] > 0 for c in (0, 1, 4, 5)) and all(t[c] == -1 for c in (2, 3, 6, 7)), t
     for ii in range(c["strn"]):
         conc, lnq, _ = ctx.get_conc(ii)
         np.testing.assert_array_equal(conc, ref[ii])
-    print("round ms (g1 four, g2 four, g1 persistent, g2 persistent)", t)
+    print("round ms", t)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_persistent_launch_of_the_shared_memory_kernels(built_lib, monkeypatch, precision):
+    """The shared-memory step kernels of the compile-time shapes as one
+    persistent launch per contour step (SCFT_PERSIST=1): a props round of four
+    64^3 replicas gives the densities and lnQ of four launches per step bit
+    for bit, with N + 6 launches per round instead of 4 N + 6."""
+    monkeypatch.delenv("SCFT_REG64", raising=False)
+    c = dict(STRING_64, N=40, strn=4)
+    wm, wp = fields(c)
+
+    def run(persist):
+        monkeypatch.setenv("SCFT_PERSIST", persist)
+        ctx = S.StringSolver(c, precision=precision)
+        for ii in range(c["strn"]):
+            ctx.set_fields(ii, wm[ii], wp[ii])
+        ctx.solve_field0_all(2, 0.0)
+        return ctx, [ctx.get_conc(ii) for ii in range(c["strn"])]
+
+    c1, one = run("1")
+    c4, four = run("0")
+    assert c4.stats()["kernel_launches"] > 3 * c1.stats()["kernel_launches"]
+    for (ca, qa, pa), (cb, qb, pb) in zip(one, four):
+        np.testing.assert_array_equal(ca, cb)
+        assert qa == qb

@@ -685,31 +685,58 @@ __device__ __noinline__ void combine_pf_call(const PropsArgs<T> *a, int s, int x
     combine_pf_body<T, MT, FM0, FM1, FM2>(*a, s, 0, x, fld, slot, smem_raw);
 }
 
+// Claim order: the (slot, field) groups form blocks of kStepBlock; wave w holds
+// phase p of block w - p for p = 3, 2, 1, 0 (the oldest work first).  Phase
+// p of a block thus comes one wave after phase p - 1 of the same block, so
+// the order respects every dependency, and the phases of different blocks
+// overlap instead of running one after another over the whole batch.
+constexpr int kStepBlock = 4;
+
+// item `it` of the claim order -> (phase, group, unit); false past the end
+__device__ __forceinline__ bool step_item(int it, int G, const int *per, int &phase, int &group, int &unit)
+{
+    const int nblk = (G + kStepBlock - 1) / kStepBlock;
+    for (int w = 0; w < nblk + 3; w++)
+        for (int p = 3; p >= 0; p--) {
+            const int b = w - p;
+            if (b < 0 || b >= nblk) continue;
+            const int g0 = b * kStepBlock, ng = min(kStepBlock, G - g0);
+            const int n = ng * per[p];
+            if (it < n) {
+                phase = p;
+                group = g0 + it / per[p];
+                unit = it - (group - g0) * per[p];
+                return true;
+            }
+            it -= n;
+        }
+    return false;
+}
+
 template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
-__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1)
     k_step_pf(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int s, int nslots)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ int item_sh, ok_sh;
+    __shared__ int item_sh[3], ok_sh;
     constexpr int ntiles = (FM1 * (FM2 / 2 + 1) + TC - 1) / TC;
     const int G = 2 * nslots;  // (slot, field) groups
     const int per[4] = {ntiles, FM0, ntiles, FM0};
-    const int total = G * (2 * ntiles + 2 * FM0);
     int *claim = a.sync + s;      // this step's claim counter
     int *done = a.sync + a.g.Ns;  // [phase][group] completion counters
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
     for (;;) {
         fence_proxy_async_smem();
-        if (threadIdx.x == 0) item_sh = atomicAdd(claim, 1);
-        __syncthreads();
-        int it = item_sh;
-        if (it >= total) break;
-        int phase = 0;
-        while (it >= G * per[phase]) {
-            it -= G * per[phase];
-            phase++;
+        if (threadIdx.x == 0) {
+            int ph = -1, gr = 0, un = 0;
+            if (!step_item(atomicAdd(claim, 1), G, per, ph, gr, un)) ph = -1;
+            item_sh[0] = ph;
+            item_sh[1] = gr;
+            item_sh[2] = un;
         }
-        const int group = it / per[phase], unit = it - group * per[phase];
+        __syncthreads();
+        const int phase = item_sh[0], group = item_sh[1], unit = item_sh[2];
+        if (phase < 0) break;
         const int slot = group >> 1, fld = group & 1;
         if (phase > 0) {
             if (threadIdx.x == 0) {

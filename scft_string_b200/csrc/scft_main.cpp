@@ -10,6 +10,10 @@
 //   precision 64 (default, the reference arithmetic) or 32 (FP32 propagator bulk)
 //   batched   1 (default): replicas advance together; 0: one at a time
 //   errtol    stop when errtot <= errtol (0 = never, as the reference)
+//   handover  with precision 32: when errtot <= handover, or after 200
+//             iterations without 1 % progress, the fields move to an FP64
+//             context and the same run continues there (0 = never); the FP32
+//             propagator's error floor then no longer limits errtol or F
 //   checkpoint 1: also write the binary FP64 checkpoint `fields.ckpt` wherever
 //             the win files are written
 //   restart   1: start from `fields.ckpt` (box and fields) instead of win files
@@ -189,7 +193,7 @@ void write_win(const std::string &fn, const double *w, long M)  // scft.cu:785-7
 
 int main(int argc, char *argv[])
 {
-    double chi = 30, f = 0.8, alpha = 0.1, phidb = 0, errtol_stop = 0;
+    double chi = 30, f = 0.8, alpha = 0.1, phidb = 0, errtol_stop = 0, handover = 0;
     int N = 60, ens = 2, readwin = 1, justFE = 0, dostring = 1, strn = 48, nsterp = 4000;
     int precision = 64, batched = 1, checkpoint = 0, restart = 0, fcont = 0;
     int m[3] = {50, 50, 50}, fix[2] = {0, 0};
@@ -220,6 +224,7 @@ int main(int argc, char *argv[])
         get("precision", precision);
         get("batched", batched);
         get("errtol", errtol_stop);
+        get("handover", handover);
         get("checkpoint", checkpoint);
         get("restart", restart);
         get("fcont", fcont);
@@ -299,8 +304,8 @@ int main(int argc, char *argv[])
                "f=%.17g strn=%d fix=%d %d dostring=%d springsteps=%d precision=%d batched=%d fcont=%d\n",
                m[0], m[1], m[2], D[0], D[1], D[2], N, alpha, ens, phidb, chi, f, strn, fix[0], fix[1], dostring,
                springsteps, precision, batched, fcont);
-        printf("dryrun run readwin=%d justFE=%d nsterp=%d errtol=%.17g checkpoint=%d restart=%d\n", readwin, justFE,
-               nsterp, errtol_stop, checkpoint, restart);
+        printf("dryrun run readwin=%d justFE=%d nsterp=%d errtol=%.17g checkpoint=%d restart=%d handover=%.17g\n",
+               readwin, justFE, nsterp, errtol_stop, checkpoint, restart, handover);
         for (int ii = 0; ii < strn; ii++) {
             double sm = 0, sp = 0;
             for (long r = 0; r < M; r++) {
@@ -356,6 +361,9 @@ int main(int argc, char *argv[])
         printf("Solving fields with %d springsteps. (procid=0)\n", springsteps);
         CHECK(scft_string_begin(ctx, -1, nsterp, errTol));
         double FEprev = 0;
+        bool fp32_phase = p.precision == SCFT_FP32 && handover > 0;
+        double best = 1e300;
+        int best_k = 0;
         for (;;) {
             scft_iter_report rep;
             int done = 0;
@@ -391,6 +399,29 @@ int main(int argc, char *argv[])
             }
             if (errtol_stop > 0 && rep.errtot <= errtol_stop) break;
             if (done) break;
+            if (fp32_phase) {
+                if (rep.errtot < 0.99 * best) {
+                    best = rep.errtot;
+                    best_k = k;
+                }
+                if (rep.errtot <= handover || k - best_k >= 200) {
+                    // the same run continues in FP64 from iteration k + 1
+                    int kk = 0;
+                    CHECK(scft_string_end(ctx, &kk));
+                    scft_problem p64 = p;
+                    p64.precision = SCFT_FP64;
+                    scft_ctx *c64 = nullptr;
+                    CHECK(scft_create(&p64, &c64));
+                    scft_status hs = scft_copy_fields(c64, ctx);
+                    scft_destroy(ctx);
+                    ctx = c64;
+                    CHECK(hs);
+                    CHECK(scft_string_resume(ctx, -1, nsterp, errTol, k + 1));
+                    printf("handover to FP64 at iteration %d, errtot %.4lE (Time: %s)\n", k + 1, rep.errtot,
+                           tistr().c_str());
+                    fp32_phase = false;
+                }
+            }
         }
         int kk = 0;
         CHECK(scft_string_end(ctx, &kk));

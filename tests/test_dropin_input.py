@@ -59,7 +59,16 @@ def test_defaults_without_input_file(exe, tmp_path):
     assert p["N"] == [60] and p["chi"] == [30] and p["f"] == [0.8] and p["alpha"] == [0.1]
     assert p["ens"] == [2] and p["phidb"] == [0] and p["strn"] == [48] and p["dostring"] == [1]
     assert run["readwin"] == [1] and run["justFE"] == [0] and run["nsterp"] == [4000]
+    assert run["handover"] == [0] and run["errtol"] == [0]
     assert p["springsteps"] == [48] and len(fl) == 48 and not fl.any()
+
+
+def test_handover_and_errtol_keys(exe, tmp_path):
+    (tmp_path / "input.dat").write_text("precision = 32\nerrtol = 1e-6\nhandover = 2.5e-4\nstrn = 1\n"
+                                        "m = 8 8 8\nreadwin = 0\n")
+    p, run, fl, out = dry_run(tmp_path)
+    assert p["precision"] == [32]
+    assert run["errtol"] == [1e-6] and run["handover"] == [2.5e-4]
 
 
 def test_keys_comments_partial_lists(exe, tmp_path):

@@ -107,3 +107,32 @@ def test_dropin_checkpoint_restart(built_lib, tmp_path):
         wa, wb = numbers((a / f"win{ii}").read_text()), numbers((b / f"win{ii}").read_text())
         assert wa.size == wb.size
         assert np.abs(wa[0::2] - wb[0::2]).max() <= 1.01e-6, ii
+
+
+def test_dropin_fp32_handover_reaches_the_fp64_answer(built_lib, tmp_path):
+    """`precision = 32` with `handover`: the program iterates in FP32, moves
+    the fields to FP64 when errtot falls below the hand-over value (or stops
+    improving), continues the same run and stops at `errtol`.  Its final free
+    energy equals that of the FP64 run to the same tolerance within 1e-6 kT
+    per chain, the FP32 path's accuracy target."""
+    name = "plain_c"
+    c = dict(load_fixture(name)["params"])
+    wm, wp = fields(c)
+    fes = {}
+    for tag, extra in (("fp64", "precision = 64\n"), ("mixed", "precision = 32\nhandover = 1e-4\n")):
+        d = tmp_path / tag
+        d.mkdir()
+        (d / "input.dat").write_text(input_dat(c) + f"strn = {c['strn']}\nnsterp = 40000\nerrtol = 1e-6\n" + extra)
+        for ii in range(c["strn"]):
+            (d / f"win{ii}").write_text(win_text(wm[ii], wp[ii]))
+        p = subprocess.run([EXE], cwd=d, capture_output=True, text=True, timeout=900)
+        assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+        last = [ln for ln in p.stdout.splitlines() if ln.startswith("error ")][-1]
+        errtot = float(last.split()[2].split("/")[0])
+        assert errtot <= 1e-6, last
+        if tag == "mixed":
+            assert "handover to FP64" in p.stdout
+        fes[tag] = numbers((d / "FEs").read_text())
+        print(tag, last)
+    F64, Fmix = fes["fp64"][1::3], fes["mixed"][1::3]
+    assert np.abs(F64 - Fmix).max() <= 1e-6

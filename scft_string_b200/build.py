@@ -28,7 +28,7 @@ NVCC = _nvcc()
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["scft_ctx.cu", "props_kernels.cu", "field_kernels.cu", "stress_kernels.cu", "noalloc.cu",
               "density_ckpt.cu", "reg64.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh", "reg64.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.h", "tma.cuh", "reg64.cuh", "step_order.cuh"]
 
 
 def _stale(target, deps):

@@ -19,6 +19,7 @@
 #include "fft.cuh"
 #include "kernels.h"
 #include "tma.cuh"
+#include "step_order.cuh"
 
 namespace scft {
 
@@ -683,34 +684,6 @@ __device__ __noinline__ void combine_pf_call(const PropsArgs<T> *a, int s, int x
                                              unsigned char *smem_raw)
 {
     combine_pf_body<T, MT, FM0, FM1, FM2>(*a, s, 0, x, fld, slot, smem_raw);
-}
-
-// Claim order: the (slot, field) groups form blocks of kStepBlock; wave w holds
-// phase p of block w - p for p = 3, 2, 1, 0 (the oldest work first).  Phase
-// p of a block thus comes one wave after phase p - 1 of the same block, so
-// the order respects every dependency, and the phases of different blocks
-// overlap instead of running one after another over the whole batch.
-constexpr int kStepBlock = 4;
-
-// item `it` of the claim order -> (phase, group, unit); false past the end
-__device__ __forceinline__ bool step_item(int it, int G, const int *per, int &phase, int &group, int &unit)
-{
-    const int nblk = (G + kStepBlock - 1) / kStepBlock;
-    for (int w = 0; w < nblk + 3; w++)
-        for (int p = 3; p >= 0; p--) {
-            const int b = w - p;
-            if (b < 0 || b >= nblk) continue;
-            const int g0 = b * kStepBlock, ng = min(kStepBlock, G - g0);
-            const int n = ng * per[p];
-            if (it < n) {
-                phase = p;
-                group = g0 + it / per[p];
-                unit = it - (group - g0) * per[p];
-                return true;
-            }
-            it -= n;
-        }
-    return false;
 }
 
 template <typename T, int MT, int FM0, int FM1, int FM2, int TC>

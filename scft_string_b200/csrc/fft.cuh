@@ -626,6 +626,78 @@ __device__ __forceinline__ void slab_pack_fixed(cplx<T> *buf)
     __syncthreads();
 }
 
+
+// ===================================================================== warp-shuffle 64-point lines
+// A 64-point line held by an octet of lanes (lane bits 0-2 = sub-lane s):
+// lane s holds x[s + 8 j], j = 0..7.  With n = s + 8 n2 and k = k1 + 8 k2,
+//   X[k1 + 8 k2] = sum_s w8^(s k2) [w64^(s k1) sum_n2 x[s + 8 n2] w8^(n2 k1)],
+// so each lane runs an 8-point DFT, multiplies by w64^(s k1), the octet
+// transposes its 8 x 8 block (lane k1 receives element k1 of every lane), and
+// each lane runs a second 8-point DFT: lane k1 then holds X[k1 + 8 k2] in
+// slot k2.  The inverse has the same shape, so a transform, a pointwise
+// multiply and the inverse transform end with lane s holding x'[s + 8 j]
+// again: no shared-memory round trip and no CTA barrier inside.
+
+// 8 x 8 transpose across the lanes of an octet by three xor exchanges: at
+// mask m, the lane without bit m swaps its element j|m with element j of the
+// lane with bit m (for every j without bit m).  Afterwards lane i holds, in
+// slot j, what lane j held in slot i.
+template <typename T>
+__device__ __forceinline__ void octet_transpose(cplx<T> (&a)[8], int s)
+{
+#pragma unroll
+    for (int m = 1; m < 8; m <<= 1) {
+        const bool up = (s & m) != 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (j & m) continue;
+            const cplx<T> send = up ? a[j] : a[j | m];
+            cplx<T> r;
+            r.x = __shfl_xor_sync(0xffffffffu, send.x, m);
+            r.y = __shfl_xor_sync(0xffffffffu, send.y, m);
+            if (up)
+                a[j] = r;
+            else
+                a[j | m] = r;
+        }
+    }
+}
+
+// w[k] = exp(-2 pi i s k / 64), k = 1..7 (w[0] unused), from the length-64
+// table tw[t] = exp(-2 pi i t / 64)
+template <typename T>
+__device__ __forceinline__ void octet_twiddles(cplx<T> (&w)[8], const cplx<T> *__restrict__ tw, int s)
+{
+    w[0] = {(T)1, (T)0};
+#pragma unroll
+    for (int k = 1; k < 8; k++) w[k] = tw[s * k];
+}
+
+// forward 64-point transform of the octet's line (sign -1): in, lane s slot j
+// = x[s + 8 j]; out, lane s slot j = X[s + 8 j]
+template <typename T>
+__device__ __forceinline__ void octet_fft64_fwd(cplx<T> (&v)[8], const cplx<T> (&w)[8], int s)
+{
+    Dft<T, 8>::run(v, -1, nullptr, 0);
+#pragma unroll
+    for (int k = 1; k < 8; k++) v[k] = cmul(v[k], w[k]);
+    octet_transpose(v, s);
+    Dft<T, 8>::run(v, -1, nullptr, 0);
+}
+
+// inverse (sign +1, unnormalised) of the same layout: in, lane s slot j =
+// X[s + 8 j]; out, lane s slot j = x[s + 8 j]
+template <typename T>
+__device__ __forceinline__ void octet_fft64_inv(cplx<T> (&v)[8], const cplx<T> (&w)[8], int s)
+{
+    Dft<T, 8>::run(v, +1, nullptr, 0);
+#pragma unroll
+    for (int k = 1; k < 8; k++) v[k] = cmulc(v[k], w[k]);
+    octet_transpose(v, s);
+    Dft<T, 8>::run(v, +1, nullptr, 0);
+}
+
+
 // packed real rows (stride M2 + 1) -> half spectrum [y][kz]
 template <typename T, int M1, int M2, int NT>
 __device__ __forceinline__ void slab_forward_fixed(cplx<T> *buf, const cplx<T> *twy, const cplx<T> *twz)
@@ -666,3 +738,4 @@ __device__ __forceinline__ void slab_inverse_fixed(cplx<T> *buf, const cplx<T> *
 }
 
 }  // namespace scft
+

@@ -61,6 +61,8 @@ struct PropsLaunch {
     int ptile_wide;  // tensor-map x pass with tiles of twice the default width
     int pencil_tma_smem_wide;
     const CUtensorMap *tmap_wide;  // the same spectra with the wide tile box
+    int pencil_sh;   // m0 = 64: x pass as register transforms with warp-shuffle transposes (k_pencil_sh);
+                     // tmap and tmap_wide are then the 128-byte-swizzled map of 128-byte boxes
     int reg;         // 64^3 FP32: register-resident step kernels (reg64.cu) instead of the shared-memory ones
     int persist;     // one persistent launch per contour step instead of four (register kernels, or the
                      // shared-memory kernels of the compile-time shapes)
@@ -79,6 +81,8 @@ int reg64_step_grid();
 void reg64_step(const PropsArgs<float> &a, int nslots, int s, int grid, cudaStream_t st);
 
 void pf_smem_bytes(int id, int fp32, int &mid, int &comb);
+// dynamic shared memory of k_pencil_sh for tiles of tc columns
+int pencil_sh_smem_bytes(int fp32, int tc, int m0);
 
 int fixed_shape_id(int m0, int m1, int m2);
 int fixed_shape_threads(int id);

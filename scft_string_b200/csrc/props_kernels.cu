@@ -609,6 +609,135 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
     pencil_tma_body<T, MT, FM0, FM1, FM2, TC>(tmap, a, both, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
+// ---------------------------------------------------------------- shuffle pencil (m0 = 64)
+// Opt-in (SCFT_PENCIL_SHUFFLE=1): on the 16-replica 64^3 string it measured
+// as fast as the Stockham pencil at the same tile width and 2 % slower than
+// its wide tiles, because in the full pipeline the x pass is bound by moving
+// the spectra, not by its barriers.
+// The x pass of the m0 = 64 shapes with the transforms in registers: each
+// column of a tile is one octet of lanes (octet_fft64_fwd / _inv), so a
+// transform, the diffusion factor and the inverse transform run without a
+// shared-memory round trip or a CTA barrier.  The tiles arrive through the
+// spectrum tensor map with 128-byte swizzling, in boxes of 128 bytes by m0
+// rows: element (x, c) of a box sits in 16-byte chunk (c-chunk XOR x mod 8)
+// of row x, so the eight lanes of an octet, which read rows s + 8 j of one
+// column, hit eight different chunks and the accesses are free of bank
+// conflicts.  Shared layout: mbarriers at 0, the x factors at 128, the
+// column factors at 640, the tiles from the next 1024-byte boundary (the
+// swizzle pattern repeats every 1024 bytes).
+template <typename T>
+struct PencilSh {
+    static constexpr int CPB = 128 / (int)sizeof(cplx<T>);  // complex elements per box row
+    static constexpr int BOXW = 128 / (int)sizeof(T);        // box width in reals
+    static constexpr int HEADER = 1024;
+    // dynamic shared memory of a tile of tc columns and m0 rows, both spectra
+    static __host__ __device__ constexpr int smem(int tc, int m0)
+    {
+        return HEADER + 1023 + 2 * tc * m0 * (int)sizeof(cplx<T>);
+    }
+    // complex index of element (x, c) of a tile
+    static __device__ __forceinline__ int at(int x, int c, int m0)
+    {
+        const int b = c / CPB, cc = c % CPB;
+        const int chunk = sizeof(T) == 4 ? cc >> 1 : cc;
+        const int sw = chunk ^ (x & 7);
+        return b * CPB * m0 + x * CPB + (sizeof(T) == 4 ? (sw << 1) | (cc & 1) : sw);
+    }
+};
+
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__device__ __forceinline__ void pencil_sh_body(const CUtensorMap &tmap, const PropsArgs<T> &a, int both, int tile,
+                                               int fld, int slot, unsigned char *smem_raw)
+{
+    static_assert(FM0 == 64, "octet transforms are 64-point");
+    using P = PencilSh<T>;
+    static_assert(TC % P::CPB == 0 && (TC % 4) == 0, "tile of whole boxes and whole warps");
+    constexpr int m0 = FM0, m1 = FM1, mk2 = FM2 / 2 + 1;
+    constexpr int NBOX = TC / P::CPB;
+    constexpr int TILE = TC * m0;  // complex elements per spectrum tile
+    constexpr uint32_t BOX_BYTES = 128u * m0;
+    constexpr int NO = MT / 8;  // octets
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    T *gx = reinterpret_cast<T *>(smem_raw + 128);
+    T *colf = reinterpret_cast<T *>(smem_raw + 640);
+    const uint32_t base = smem_addr(smem_raw + P::HEADER);
+    cplx<T> *buf0 = reinterpret_cast<cplx<T> *>(smem_raw + P::HEADER + ((1024u - (base & 1023u)) & 1023u));
+    const int ncol = m1 * mk2, c0 = tile * TC;
+    const int x0 = 2 * c0;
+    const int y0 = (((a.slot0 + slot) * 2 + fld) * 2) * m0;
+    const int npass = both ? 2 : 1;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+        for (int p = 0; p < npass; p++) {
+            mbar_expect_tx(&bars[p], NBOX * BOX_BYTES);
+            for (int b = 0; b < NBOX; b++)
+                tma_load_2d(buf0 + p * TILE + b * P::CPB * m0, &tmap, x0 + b * P::BOXW, y0 + p * m0, &bars[p]);
+        }
+    }
+    const T *kf = a.kfac + (size_t)a.slot_rep[slot] * a.kf_stride;  // the replica's box
+    for (int i = threadIdx.x; i < m0; i += MT) gx[i] = kf[i];
+    for (int t = threadIdx.x; t < TC; t += MT) {
+        const int c = c0 + t;
+        const int yy = c / mk2, kz = c - yy * mk2;
+        colf[t] = c < ncol ? kf[m0 + yy] * kf[m0 + m1 + kz] : (T)0;
+    }
+    const int s = threadIdx.x & 7, oct = threadIdx.x >> 3;
+    cplx<T> w[8];
+    octet_twiddles(w, a.tw, s);
+    __syncthreads();
+    const T invM = a.invM, Mreal = a.Mreal;
+    const int nlines = npass * TC;
+    int stored = 0;  // spectra whose tiles have been stored
+#pragma unroll 1
+    for (int l0 = 0; l0 < nlines; l0 += NO) {
+        const int line = l0 + oct;
+        if (line < nlines) {  // whole warps: nlines and NO are multiples of 4 octets
+            const int pass = line / TC, t = line - pass * TC;
+            cplx<T> *buf = buf0 + pass * TILE;
+            mbar_wait(&bars[pass], 0, a.err);
+            cplx<T> v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = buf[P::at(s + 8 * j, t, m0)];
+            octet_fft64_fwd(v, w, s);
+            // bin s + 8 j of column t: pass 0: K2 = g/M ; pass 1: K1 = g^2/M
+            // (Prepare_dev_expKsq2_expKsq, GPU_kernels.h:207-213)
+            const T ct = colf[t];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const T k2 = gx[s + 8 * j] * ct;
+                const T f = pass == 0 ? k2 * invM : (k2 * invM) * (k2 * invM) * Mreal;
+                v[j].x *= f;
+                v[j].y *= f;
+            }
+            octet_fft64_inv(v, w, s);
+#pragma unroll
+            for (int j = 0; j < 8; j++) buf[P::at(s + 8 * j, t, m0)] = v[j];
+        }
+        // spectra completed by this round of lines leave through tile stores
+        const int done = min(npass, (l0 + NO) / TC);
+        if (done > stored) {
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int p = stored; p < done; p++)
+                    for (int b = 0; b < NBOX; b++)
+                        tma_store_2d(&tmap, x0 + b * P::BOXW, y0 + p * m0, buf0 + p * TILE + b * P::CPB * m0);
+            stored = done;
+        }
+    }
+    if (threadIdx.x == 0) tma_store_wait_read();
+}
+
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
+    k_pencil_sh(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int both)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    pencil_sh_body<T, MT, FM0, FM1, FM2, TC>(tmap, a, both, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
 template <typename T, int MT, int FM0, int FM1, int FM2>
 __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1) k_mid_pf(PropsArgs<T> a, int s)
 {
@@ -673,6 +802,13 @@ __device__ __noinline__ void pencil_tma_call(const CUtensorMap *tmap, const Prop
     pencil_tma_body<T, MT, FM0, FM1, FM2, TC>(*tmap, *a, both, tile, fld, slot, smem_raw);
 }
 
+template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
+__device__ __noinline__ void pencil_sh_call(const CUtensorMap *tmap, const PropsArgs<T> *a, int both, int tile,
+                                            int fld, int slot, unsigned char *smem_raw)
+{
+    if constexpr (FM0 == 64) pencil_sh_body<T, MT, FM0, FM1, FM2, TC>(*tmap, *a, both, tile, fld, slot, smem_raw);
+}
+
 template <typename T, int MT, int FM0, int FM1, int FM2>
 __device__ __noinline__ void mid_pf_call(const PropsArgs<T> *a, int s, int x, int fld, int slot, unsigned char *smem_raw)
 {
@@ -688,7 +824,7 @@ __device__ __noinline__ void combine_pf_call(const PropsArgs<T> *a, int s, int x
 
 template <typename T, int MT, int FM0, int FM1, int FM2, int TC>
 __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1)
-    k_step_pf(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int s, int nslots)
+    k_step_pf(const __grid_constant__ CUtensorMap tmap, PropsArgs<T> a, int s, int nslots, int sh)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ int item_sh[3], ok_sh;
@@ -729,7 +865,10 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 4 : 2) : 1)
         }
         int nbar;
         if (phase == 0 || phase == 2) {
-            pencil_tma_call<T, MT, FM0, FM1, FM2, TC>(&tmap, &a, phase == 0, unit, fld, slot, smem_raw);
+            if (sh)
+                pencil_sh_call<T, MT, FM0, FM1, FM2, TC>(&tmap, &a, phase == 0, unit, fld, slot, smem_raw);
+            else
+                pencil_tma_call<T, MT, FM0, FM1, FM2, TC>(&tmap, &a, phase == 0, unit, fld, slot, smem_raw);
             nbar = 2;
             if (threadIdx.x == 0) {
                 bulk_wait_all();  // the tile stores have reached global memory
@@ -1024,6 +1163,17 @@ void launch_pencil(const PropsArgs<T> &a, const PropsLaunch &L, dim3 gp, int bot
             // tile width: kTile columns, or twice that (two butterflies per
             // thread between barriers) when the autotuner picked it
             constexpr int TC = kTile<T>::value, ncol = F1 * (F2 / 2 + 1);
+            if constexpr (F0 == 64) {
+                if (L.pencil_sh) {
+                    if (L.ptile_wide)
+                        k_pencil_sh<T, MT, F0, F1, F2, 2 * TC><<<dim3((ncol + 2 * TC - 1) / (2 * TC), gp.y, gp.z), MT,
+                                                                 L.pencil_tma_smem_wide, st>>>(*L.tmap_wide, a, both);
+                    else
+                        k_pencil_sh<T, MT, F0, F1, F2, TC><<<dim3((ncol + TC - 1) / TC, gp.y, gp.z), MT,
+                                                             L.pencil_tma_smem, st>>>(*L.tmap, a, both);
+                    return;
+                }
+            }
             if (L.ptile_wide)
                 k_pencil_tma<T, MT, F0, F1, F2, 2 * TC><<<dim3((ncol + 2 * TC - 1) / (2 * TC), gp.y, gp.z), MT,
                                                           L.pencil_tma_smem_wide, st>>>(*L.tmap_wide, a, both);
@@ -1060,10 +1210,11 @@ int launch_props_mt(const PropsArgs<T> &a, const PropsLaunch &L, int nslots, cud
             launch_combine<T, MT, F0, F1, F2>(a, L, gs, -1, 1, st);
             for (int s = 0; s < g.Ns; s++) {
                 if (L.ptile_wide)
-                    k_step_pf<T, MT, F0, F1, F2, 2 * TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(*L.tmap_wide, a, s,
-                                                                                                    nslots);
+                    k_step_pf<T, MT, F0, F1, F2, 2 * TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(
+                        *L.tmap_wide, a, s, nslots, L.pencil_sh);
                 else
-                    k_step_pf<T, MT, F0, F1, F2, TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(*L.tmap, a, s, nslots);
+                    k_step_pf<T, MT, F0, F1, F2, TC><<<L.step_grid_pf, MT, L.step_pf_smem, st>>>(*L.tmap, a, s, nslots,
+                                                                                                L.pencil_sh);
             }
             n += g.Ns;
         }
@@ -1131,6 +1282,14 @@ int set_smem_mt(const PropsLaunch &L)
             e4 = raise_dyn_smem(k_pencil_tma<T, MT, F0, F1, F2, kTile<T>::value>, L.pencil_tma_smem);
             if (e4 == cudaSuccess && L.tmap_wide)
                 e4 = raise_dyn_smem(k_pencil_tma<T, MT, F0, F1, F2, 2 * kTile<T>::value>, L.pencil_tma_smem_wide);
+            if constexpr (F0 == 64) {
+                if (e4 == cudaSuccess && L.pencil_sh) {
+                    e4 = raise_dyn_smem(k_pencil_sh<T, MT, F0, F1, F2, kTile<T>::value>, L.pencil_tma_smem);
+                    if (e4 == cudaSuccess && L.tmap_wide)
+                        e4 = raise_dyn_smem(k_pencil_sh<T, MT, F0, F1, F2, 2 * kTile<T>::value>,
+                                            L.pencil_tma_smem_wide);
+                }
+            }
         }
         if (e4 == cudaSuccess && L.pf) {
             e4 = raise_dyn_smem(k_combine_pf<T, MT, F0, F1, F2>, L.combine_pf_smem);
@@ -1174,6 +1333,11 @@ void pf_smem_bytes(int id, int fp32, int &mid, int &comb)
         pf_smem<float>(id, mid, comb);
     else
         pf_smem<double>(id, mid, comb);
+}
+
+int pencil_sh_smem_bytes(int fp32, int tc, int m0)
+{
+    return fp32 ? PencilSh<float>::smem(tc, m0) : PencilSh<double>::smem(tc, m0);
 }
 
 // op 0: props, 1: single step, 2: shared-memory attributes, 3: chain segment, 4: CTAs of the

@@ -776,19 +776,26 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
                 cuuint64_t dims[2] = {(cuuint64_t)2 * g.m1 * g.mk2, (cuuint64_t)S * 2 * 2 * g.m0};
                 cuuint64_t strides[1] = {(cuuint64_t)2 * g.m1 * g.mk2 * T};
                 cuuint32_t es[2] = {1, 1};
+                // m0 = 64 with SCFT_PENCIL_SHUFFLE=1: the shuffle pencil, which reads 128-byte boxes
+                // with 128-byte swizzling (opt-in: it measured no faster than the Stockham pencil)
+                const char *shv = getenv("SCFT_PENCIL_SHUFFLE");
+                L.pencil_sh = g.m0 == 64 && shv && shv[0] == '1';
                 auto encode = [&](CUtensorMap *m, int w) {
-                    cuuint32_t box[2] = {(cuuint32_t)(2 * w), (cuuint32_t)g.m0};
+                    cuuint32_t box[2] = {(cuuint32_t)(L.pencil_sh ? 128 / T : 2 * w), (cuuint32_t)g.m0};
                     return ((EncodeFn)fn)(m, T == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
                                           ctx->spec, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                                          L.pencil_sh ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
                 };
-                auto smem_for = [&](int w) { return (int)(128 + (2 * w * g.m0 + g.m0) * 2 * T + (w + g.m0) * T); };
+                auto smem_for = [&](int w) {
+                    return L.pencil_sh ? pencil_sh_smem_bytes(T == 4, w, g.m0)
+                                       : (int)(128 + (2 * w * g.m0 + g.m0) * 2 * T + (w + g.m0) * T);
+                };
                 if (encode(&ctx->tmap, tc) == CUDA_SUCCESS && g.m0 <= 256 && (strides[0] % 16) == 0) {
                     L.tma_pencil = 1;
                     L.tmap = &ctx->tmap;
                     L.pencil_tma_smem = smem_for(tc);
-                    // the wide tile (2 tc columns; box width 4 tc reals <= 256)
+                    // the wide tile (2 tc columns; box width 4 tc reals <= 256, or 4 boxes of the swizzled map)
                     if (4 * tc <= 256 && smem_for(2 * tc) <= (int)prop.sharedMemPerBlockOptin &&
                         encode(&ctx->tmap_wide, 2 * tc) == CUDA_SUCCESS) {
                         L.tmap_wide = &ctx->tmap_wide;
@@ -796,6 +803,7 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
                         if (const char *ev = getenv("SCFT_PENCIL_TILE_WIDE")) L.ptile_wide = ev[0] == '1';
                     }
                 }
+                if (!L.tma_pencil) L.pencil_sh = 0;
             }
         }
         // the persistent step kernel of the compile-time shapes runs all three
@@ -811,8 +819,6 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
             rc = SCFT_CUDA_ERROR;
             goto done;
         }
-        // register kernels: one persistent launch per contour step unless SCFT_NO_PERSIST=1
-        // (scft_autotune compares it with four launches per step)
         // one persistent launch per contour step: the register kernels start with
         // it, the shared-memory kernels with four launches (scft_autotune compares
         // both); SCFT_PERSIST=0|1 sets the start, SCFT_NO_PERSIST=1 rules it out

@@ -160,3 +160,40 @@ def test_register_kernels_64cubed_fp32(built_lib, monkeypatch, persist):
     lnQ0, phis0 = O.Density(m, D, Ns).props(w0, Ns, 0.1, 0.8, f, 2)
     assert abs(lnQ - lnQ0) <= 1e-5 * abs(lnQ0)
     assert np.abs(conc - w0[2 * M:]).max() <= 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("wide", ["0", "1"])
+def test_shuffle_pencil_m0_64(built_lib, monkeypatch, prec, wide):
+    """The x pass as octet register transforms with warp-shuffle transposes
+    (SCFT_PENCIL_SHUFFLE=1, grids with m0 = 64), at both tile widths: steps
+    against the FP64 oracle at the step tolerance of the precision, and a
+    props round with one persistent launch per contour step equal bit for bit
+    to one with four launches, both against the oracle's lnQ."""
+    monkeypatch.setenv("SCFT_PENCIL_SHUFFLE", "1")
+    monkeypatch.setenv("SCFT_PENCIL_TILE_WIDE", wide)
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    Ns, f = 16, 0.5
+    for m, D in [((64, 64, 64), (4.0, 4.0, 4.0)), ((64, 64, 96), (4.0, 4.0, 6.0))]:
+        M = int(np.prod(m))
+        wm, wp = fields(m, 11, 1.0)
+        od = O.Density(m, D, Ns)
+        od.prepare(1.0 / Ns, np.concatenate([wm, wp]))
+        qin = 1.0 + 0.3 * np.random.default_rng(4).normal(size=2 * M)
+        res = []
+        for persist in ("0", "1"):
+            monkeypatch.setenv("SCFT_PERSIST", persist)
+            ctx = S.Context(m, D, Ns, chi=10, f=f, phidb=0.8, ens=2, strn=1, dostring=0, precision=prec)
+            ctx.set_fields(0, wm, wp)
+            if persist == "0":
+                for s in [0, 7, 8, Ns - 1]:
+                    ref = od.do_step(qin, s, 8, 8)
+                    got = ctx.do_step(0, qin, s)
+                    assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (m, s)
+            ctx.props(0)
+            res.append(ctx.get_conc(0))
+        assert np.array_equal(res[0][0], res[1][0]) and res[0][1] == res[1][1], m
+        w0 = np.zeros(6 * M)
+        w0[:M], w0[M:2 * M] = wm, wp
+        lnQ0, _ = O.Density(m, D, Ns).props(w0, Ns, 0.1, 0.8, f, 2)
+        assert abs(res[0][1] - lnQ0) <= (1e-12 if prec == "fp64" else 1e-5) * abs(lnQ0), m

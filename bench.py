@@ -676,7 +676,7 @@ def run_ours(a, cfg, rank, world, dev):
                e2e_same_iterations=same,
                schedule={"slot_groups": groups, "wide_pencil_tiles": bool(wide),
                          "persistent_step_launch": bool(persist),
-                         "props_round_ms": {f"g{1 + (c & 1)}_tile{1 + ((c >> 1) & 1)}_{'persistent' if c >> 2 else 'four'}":
+                         "props_round_ms": {f"g{1 << (c % 3)}_tile{1 + (c // 3) % 2}_{'persistent' if c >= 6 else 'four'}":
                                             v for c, v in enumerate(tune_ms) if v > 0}})
     # ---- the other precision (batched) and plain FP64 on the same window
     if rank == 0 and world == 1 and not a.no_fp64:

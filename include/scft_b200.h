@@ -286,10 +286,14 @@ scft_status scft_checkpoint_info(const char *path, int *version, int *strn, int 
  * not available (any pointer may be NULL).  Performance-only: results do not
  * depend on the setting. */
 scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms);
-/* scft_autotune over a third axis as well: four launches per contour step, or
- * one persistent launch per step (work items claimed in order, bounded
- * waits), where the context has one (compile-time grid shapes).  times_ms[c]
- * for c = (groups - 1) + 2 wide + 4 persist, -1 where not available;
+/* scft_autotune over more schedules: 1, 2 or 4 slot groups (four groups run
+ * two after another on each of the two streams, so fewer spectra are live
+ * at once; only with at least 16 replicas, and batches of fewer than 16
+ * replicas then run as 2 groups), the two tile widths, and four
+ * launches per contour step or one persistent launch per step (work items
+ * claimed in order, bounded waits) where the context has one (compile-time
+ * grid shapes).  times_ms[12]: times_ms[c] for c = gi + 3 wide + 6 persist
+ * with gi = 0, 1, 2 for 1, 2, 4 groups, -1 where not available;
  * *persist_out = the launch form kept.  Performance-only: results do not
  * depend on the setting. */
 scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int *persist_out, double *times_ms);

@@ -466,10 +466,10 @@ class Context:
 
     def autotune(self):
         """(slot groups kept, wide pencil tiles kept, persistent step launch kept,
-        best props-round times in ms indexed (groups - 1) + 2 wide + 4 persistent;
-        -1 where not available)."""
+        best props-round times in ms indexed gi + 3 wide + 6 persistent with
+        gi = 0, 1, 2 for 1, 2, 4 slot groups; -1 where not available)."""
         g, w, p = C.c_int(), C.c_int(), C.c_int()
-        t = np.zeros(8)
+        t = np.zeros(12)
         self._ck(lib().scft_autotune_ex(self.h, C.byref(g), C.byref(w), C.byref(p), _p(t)))
         return g.value, w.value, p.value, [float(v) for v in t]
 

@@ -24,6 +24,9 @@
 
 using namespace scft;
 
+// schedules scft_autotune_ex times: slot groups (1, 2, 4) x tile width x launch form
+constexpr int kTuneCandidates = 12;
+
 namespace {
 
 constexpr int kRedBlocks = 148;  // reduction grid: one block per SM
@@ -174,7 +177,7 @@ PropsArgs<T> props_args(scft_ctx *ctx, const int *slot_rep)
 // the same arguments for the slots [s0, s0 + n) of a round: every per-slot
 // base pointer moves by s0 slots
 template <typename T>
-PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0)
+PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0, int lane = 0)
 {
     PropsArgs<T> a = props_args<T>(ctx, slot_rep + s0);
     const size_t M = ctx->M, Mk = ctx->Mk;
@@ -185,7 +188,7 @@ PropsArgs<T> props_args_from(scft_ctx *ctx, const int *slot_rep, int s0)
     a.partials += (size_t)s0 * ctx->npart_stride;
     a.slot0 = s0;
     if (a.jtab) a.jtab += (size_t)s0 * M;
-    if (a.sync && s0 > 0) a.sync += ctx->sync_stride;  // the second slot group's counters
+    if (a.sync && lane) a.sync += ctx->sync_stride;  // counters of the groups on the second stream
     return a;
 }
 
@@ -232,6 +235,17 @@ scft_status upload_list(scft_ctx *ctx, const std::vector<int> &reps)
 
 scft_status props_ckpt_impl(scft_ctx *ctx, int ii, int K, double *lnQ_out, double *phis_out, double *bytes_out);
 
+// Slot groups of a batch of nb replicas: the configured count, halved while a
+// group of more than two would get fewer than 4 replicas (a launch of 2 or 3
+// replicas leaves most SMs idle: the W+ relaxation runs many such partial
+// batches), and 1 when there are fewer than 2 replicas per group.
+int effective_groups(int ngroups, int nb)
+{
+    int ng = ngroups;
+    while (ng > 2 && nb < 4 * ng) ng /= 2;
+    return (ng > 1 && nb >= 2 * ng) ? ng : 1;
+}
+
 // density::props for a list of replicas; scalars land in ctx->rs_h.  Without a
 // full store (nostore) each replica runs from checkpoints.
 scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
@@ -263,8 +277,10 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
     for (size_t c0 = 0; c0 < reps.size(); c0 += ctx->nslots) {
         const int nb = (int)std::min<size_t>(ctx->nslots, reps.size() - c0);
         // groups of slots run as independent chains on two streams, so the
-        // last wave of one group's launch overlaps the other group's work
-        const int ng = (ctx->ngroups > 1 && nb >= 2 * ctx->ngroups) ? ctx->ngroups : 1;
+        // last wave of one group's launch overlaps the other group's work;
+        // with more than two groups each stream runs its groups one after
+        // another (fewer spectra live at once)
+        const int ng = effective_groups(ctx->ngroups, nb);
         auto launch = [&]() {
             int n = 0;
             if (ng > 1) {
@@ -275,9 +291,11 @@ scft_status props_list(scft_ctx *ctx, const std::vector<int> &reps)
                 const int s0 = nb * gi / ng, s1 = nb * (gi + 1) / ng;
                 cudaStream_t sg = (gi % 2 == 0) ? ctx->st : ctx->st2;
                 if (ctx->prec == SCFT_FP32)
-                    n += launch_props<float>(props_args_from<float>(ctx, ctx->rep_dev + c0, s0), ctx->L, s1 - s0, sg);
+                    n += launch_props<float>(props_args_from<float>(ctx, ctx->rep_dev + c0, s0, gi % 2), ctx->L,
+                                             s1 - s0, sg);
                 else
-                    n += launch_props<double>(props_args_from<double>(ctx, ctx->rep_dev + c0, s0), ctx->L, s1 - s0, sg);
+                    n += launch_props<double>(props_args_from<double>(ctx, ctx->rep_dev + c0, s0, gi % 2), ctx->L,
+                                              s1 - s0, sg);
             }
             if (ng > 1) {
                 cudaEventRecord(ctx->join, ctx->st2);
@@ -719,7 +737,7 @@ scft_status scft_create(const scft_problem *p, scft_ctx **out)
         CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
         CKC(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
         CKC(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
-        if (const char *ev = getenv("SCFT_GROUPS")) ctx->ngroups = std::max(1, std::min(2, atoi(ev)));
+        if (const char *ev = getenv("SCFT_GROUPS")) ctx->ngroups = std::max(1, std::min(8, atoi(ev)));
         CKC(cudaEventCreate(&ctx->ev0));
         CKC(cudaEventCreate(&ctx->ev1));
         for (auto &e : ctx->tev) CKC(cudaEventCreate(&e));
@@ -2226,9 +2244,11 @@ scft_status scft_reset_stats(scft_ctx *ctx)
     return SCFT_OK;
 }
 
-// Times props rounds of every replica for each schedule -- one or two
-// concurrent slot groups, x-pencil tiles of the default or twice the width
-// (when the grid has tensor-map pencils) -- and keeps the fastest.  Each
+// Times props rounds of every replica for each schedule -- one, two or four
+// slot groups (two concurrent streams; four groups run two after another on
+// each), x-pencil tiles of the default or twice the width (when the grid has
+// tensor-map pencils), four launches or one persistent launch per contour
+// step -- and keeps the fastest.  Each
 // candidate re-captures its graphs, runs one untimed round, then the best of
 // three timed rounds counts.  The rounds recompute every replica's densities
 // at its current fields, so the state a caller sees afterwards is unchanged;
@@ -2237,7 +2257,7 @@ scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int 
 {
     if (!ctx) return SCFT_BAD_INPUT;
     if (times_ms)
-        for (int c = 0; c < 8; c++) times_ms[c] = -1;
+        for (int c = 0; c < kTuneCandidates; c++) times_ms[c] = -1;
     if (ctx->nostore) {  // props run one replica at a time from checkpoints: nothing to schedule
         if (groups_out) *groups_out = 1;
         if (wide_out) *wide_out = ctx->L.ptile_wide;
@@ -2257,14 +2277,15 @@ scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int 
     double best = 0;
     int best_g = 1, best_w = 0, best_p = 0;
     bool first = true;
-    // axes: slot groups (1, 2) x x-pencil tile width (default, wide; tensor-map
-    // pencils of the shared-memory kernels only) x launches per contour step
-    // (four, or one persistent launch)
+    // axes: slot groups (1, 2, 4) x x-pencil tile width (default, wide;
+    // tensor-map pencils of the shared-memory kernels only) x launches per
+    // contour step (four, or one persistent launch); c = gi + 3 wide + 6 persist
     const int nw = (!ctx->L.reg && ctx->L.tmap_wide) ? 2 : 1;
     const int np = ctx->persist_ok ? 2 : 1;
-    for (int c = 0; c < 8; c++) {
-        const int ng = 1 + (c & 1), wide = (c >> 1) & 1, persist = c >> 2;
+    for (int c = 0; c < kTuneCandidates; c++) {
+        const int ng = 1 << (c % 3), wide = (c / 3) & 1, persist = c / 6;
         if (wide >= nw || persist >= np) continue;
+        if (effective_groups(ng, (int)all.size()) != ng) continue;  // props_list would run fewer groups
         drop_graphs();
         ctx->ngroups = ng;
         ctx->L.ptile_wide = wide;
@@ -2300,10 +2321,14 @@ scft_status scft_autotune_ex(scft_ctx *ctx, int *groups_out, int *wide_out, int 
 
 scft_status scft_autotune(scft_ctx *ctx, int *groups_out, int *wide_out, double *times_ms)
 {
-    double t8[8];
-    scft_status s = scft_autotune_ex(ctx, groups_out, wide_out, nullptr, t8);
-    if (times_ms)
-        for (int c = 0; c < 4; c++) times_ms[c] = t8[c];
+    double t[kTuneCandidates];
+    scft_status s = scft_autotune_ex(ctx, groups_out, wide_out, nullptr, t);
+    if (times_ms) {  // four launches per step: (1, default), (2, default), (1, wide), (2, wide)
+        times_ms[0] = t[0];
+        times_ms[1] = t[1];
+        times_ms[2] = t[3];
+        times_ms[3] = t[4];
+    }
     return s;
 }
 

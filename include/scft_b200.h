@@ -240,9 +240,10 @@ scft_status scft_spline_redist(scft_ctx *ctx, const double *x, const double *xre
  * [q(s+1), q^dagger(s+1)], each 2*M doubles; f is the A fraction (0..1) as in
  * scft_problem; stream may be NULL.  Limits: FP64, M <= 32768, each m_i <= 64
  * (BAD_INPUT beyond).  The first call on a device looks up the array's
- * address (cudaGetSymbolAddress): make it before any stream capture.  Calls
- * share the array, so calls that overlap on the GPU race; the call waits for
- * its stream before returning. */
+ * address (cudaGetSymbolAddress).  Calls share the array, so calls that
+ * overlap on the GPU race.  The call reads the kernels' error word back to
+ * the host and waits for its stream before returning, so it cannot be
+ * recorded into a CUDA graph. */
 scft_status scft_do_step_noalloc(const int *m, const double *D, int N, double f, const double *w2M,
                                  const double *in2M, double *out2M, int s, void *stream);
 

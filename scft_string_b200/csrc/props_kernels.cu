@@ -621,8 +621,8 @@ __global__ void __launch_bounds__(MT, MT == 256 ? (sizeof(T) == 4 ? 3 : 2) : 1)
 // spectrum tensor map with 128-byte swizzling, in boxes of 128 bytes by m0
 // rows: element (x, c) of a box sits in 16-byte chunk (c-chunk XOR x mod 8)
 // of row x, so the eight lanes of an octet, which read rows s + 8 j of one
-// column, hit eight different chunks and the accesses are free of bank
-// conflicts.  Shared layout: mbarriers at 0, the x factors at 128, the
+// column, hit eight different chunks (ncu still counts about a fifth of the
+// FP32 tile wavefronts as bank conflicts).  Shared layout: mbarriers at 0, the x factors at 128, the
 // column factors at 640, the tiles from the next 1024-byte boundary (the
 // swizzle pattern repeats every 1024 bytes).
 template <typename T>

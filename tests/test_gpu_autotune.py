@@ -101,3 +101,33 @@ def test_persistent_launch_of_the_shared_memory_kernels(built_lib, monkeypatch, 
     for (ca, qa, pa), (cb, qb, pb) in zip(one, four):
         np.testing.assert_array_equal(ca, cb)
         assert qa == qb
+
+
+@pytest.mark.parametrize("persist", ["0", "1"])
+def test_four_slot_groups_match_two(built_lib, monkeypatch, persist):
+    """Four slot groups (two after another on each of the two streams) change
+    only the schedule: a props round of 16 replicas, and the W+ relaxation's
+    partial batches that fall back to two groups, give the densities and lnQ
+    of two groups bit for bit, with four launches per step and with the
+    persistent launch (whose counters are per stream)."""
+    monkeypatch.delenv("SCFT_REG64", raising=False)
+    monkeypatch.setenv("SCFT_PERSIST", persist)
+    c = dict(STRING_64, m=(32, 32, 32), D=(4.0, 4.0, 4.0), N=40, strn=16)
+    wm, wp = fields(c)
+
+    def run(groups):
+        monkeypatch.setenv("SCFT_GROUPS", groups)
+        ctx = S.StringSolver(c, precision="fp32")
+        for ii in range(c["strn"]):
+            ctx.set_fields(ii, wm[ii], wp[ii])
+        k = ctx.solve_field0_all(30, 1e-4)
+        return k, [ctx.get_conc(ii) for ii in range(c["strn"])], [ctx.get_fields(ii) for ii in range(c["strn"])]
+
+    k4, conc4, w4 = run("4")
+    k2, conc2, w2 = run("2")
+    assert list(k4) == list(k2)
+    for (ca, qa, _), (cb, qb, _) in zip(conc4, conc2):
+        np.testing.assert_array_equal(ca, cb)
+        assert qa == qb
+    for a, b in zip(w4, w2):
+        np.testing.assert_array_equal(a, b)

@@ -140,6 +140,31 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def alu_peak_tflops(precision, sms=None, sm_mhz=None):
+    """Nominal non-tensor peak of the precision's pipe: SMs x FMA lanes per SM
+    (128 FP32, 64 FP64 on sm_100) x 2 flops x the maximum SM clock.
+    MEASURED_PEAKS.json has no FP32 or FP64 ALU figure, so this one is
+    computed, not measured; the SM count comes from the device (148 when none
+    is visible) and the clock from MEASURED_PEAKS.json (1965 MHz otherwise)."""
+    if sms is None:
+        sms = 148
+        try:
+            import torch
+            if torch.cuda.is_available():
+                sms = torch.cuda.get_device_properties(0).multi_processor_count
+        except Exception:
+            pass
+    if sm_mhz is None:
+        sm_mhz = 1965.0
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                sm_mhz = float(json.load(fh).get("sm_max_mhz", sm_mhz))
+        except (OSError, ValueError):
+            pass
+    lanes = 128 if precision == "fp32" else 64
+    return sms * lanes * 2 * sm_mhz * 1e6 / 1e12
+
+
 def profiled_traffic(precision="fp32"):
     """DRAM bytes per replica contour step from the committed ncu summary of
     the precision's step kernels (None when no capture was summarised)."""
@@ -811,7 +836,13 @@ def main():
                      "traffic": traffic,
                      "unit_of_work": "replica contour step (q and q^dagger advanced by ds)",
                      "algorithmic_bytes_per_unit": step_bytes,
-                     "fp32_tflops" if b == 4 else "fp64_tflops": flops},
+                     "fp32_tflops" if b == 4 else "fp64_tflops": flops,
+                     "alu": {"achieved": flops, "peak": alu_peak_tflops(a.precision), "unit": "TFLOP/s",
+                             "frac": flops / alu_peak_tflops(a.precision), "peak_kind": "nominal",
+                             "flops_per_unit": 30 * M * math.log2(M),
+                             "note": "30 M log2 M algorithmic FFT flops per replica contour step against "
+                                     "SMs x FMA lanes x 2 x max SM clock of the path's precision"},
+                     "max_frac": max(achieved / peak, flops / alu_peak_tflops(a.precision))},
         "e2e": {"value": world * a.steps / (r["e2e_ms"] / 1e3), "unit": "string iters/s",
                 "h2d_bytes_per_step": cfg["strn"] * 2 * M * 8,
                 "d2h_bytes_per_step": cfg["strn"] * 2 * M * 8,

@@ -69,3 +69,9 @@ def test_cpu_step_rate_matches_the_oracle_step():
     q1 = s.do_step(np.ones(2 * M), 0, 10, 10)
     np.testing.assert_allclose(q1[:M], d.q(0, 1), rtol=1e-14)
     np.testing.assert_allclose(q1[M:], d.q(1, 1), rtol=1e-14)
+
+
+def test_alu_peak_is_sms_times_lanes_times_clock():
+    # B200: 148 SMs at 1965 MHz: 74.4 TFLOP/s FP32 and 37.2 FP64 (non-tensor, nominal)
+    assert bench.alu_peak_tflops("fp32", sms=148, sm_mhz=1965.0) == pytest.approx(74.4457, rel=1e-4)
+    assert bench.alu_peak_tflops("fp64", sms=148, sm_mhz=1965.0) == pytest.approx(37.2229, rel=1e-4)
